@@ -1,0 +1,316 @@
+"""Benchmark: fwd+bwd+Adam training steps/s of the reference-default fitter
+(1280x720 procedural target, 60000 splats, SH degree 0, 16x16 tiles, L2 loss,
+Adam) on one B200, through the fused graph-captured step of libdiffsplat_b200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank fits its own independent
+instance (replicas: the path has no data exchange), so scaling is weak and the
+job value is the sum over ranks of steps / max-over-ranks time.
+L2 hygiene: a 256 MiB buffer is overwritten between timed steps, outside the
+timed events, so every step starts with a cold 126 MB L2.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fwd+bwd+Adam steps/s (reference-default fitter, 1280x720, 60000 splats)"
+FLUSH_BYTES = 256 << 20
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 3 + k and r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup(gpus: int):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def kernels_per_step(tiles: int) -> int:
+    passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
+    # step_begin, preprocess, 4 depth passes x 3, scan x 3, emit, tile passes x 3,
+    # ranges, composite fwd, composite bwd, backward+Adam
+    return 2 + 12 + 3 + 1 + 3 * passes + 1 + 3
+
+
+def stage_bytes(n: int, isects: int, pixels: int, tiles: int) -> dict:
+    """Algorithmic HBM bytes per launch of each stage (FP32 storage, SH 0)."""
+    passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
+    return {
+        "preprocess": n * (14 * 4 + 48 + 4 + 8 + 4 + 4),
+        "depth_sort": 4 * n * 16,
+        "scan_emit": n * 16 + isects * 8,
+        "tile_sort_ranges": passes * isects * 16 + isects * 8,
+        "composite_fwd": isects * (4 + 48) + pixels * (12 + 12 + 4 + 4),
+        "composite_bwd": isects * (4 + 4 + 52 + 36) + pixels * (12 + 12 + 4 + 4),
+        "backward_adam": n * (14 * 4 * 6) + isects * 36,
+    }
+
+
+def cpu_baseline_oracle(prob) -> dict:
+    """FP64 oracle: one fwd+bwd (+ Adam) step of the same workload on all host cores."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    P = prob.params.astype(np.float64)
+    t0 = time.perf_counter()
+    fw, gp = O.loss_and_grads(P, prob.sh_degree, prob.cam, prob.pv, prob.width, prob.height,
+                              prob.target, threads=threads)
+    m = np.zeros_like(P)
+    O.adam(P, gp, m, m.copy(), 1e-3, 1)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": "1 fwd+bwd+Adam step of the same 1280x720 / 60000-splat workload "
+                      f"({dt:.2f} s)"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from diffsplat_b200 import api
+    from diffsplat_b200.scenes import reference_default, psnr_from_ref_loss
+
+    prob = reference_default(seed=rank)
+    n = prob.params.shape[1]
+    f = api.Fitter(prob.width, prob.height, n, prob.sh_degree, lrs=prob.lrs)
+    f.set_params(prob.params)
+    f.set_target(torch.tensor(prob.target, device="cuda"))
+    f.set_camera(prob.pv, prob.cam)
+    flush = torch.empty(FLUSH_BYTES // 4, device="cuda")
+    for _ in range(args.warmup):
+        f.step(1)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            f.step(1)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_max = max_over_ranks(world, t_ms)
+    loss = f.loss()
+    # end to end through the public API: camera upload, step, loss readback each step
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e2e_ev[k][0].record()
+        f.set_camera(prob.pv, prob.cam)
+        f.step(1)
+        f.loss()
+        e2e_ev[k][1].record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, sum(a.elapsed_time(b) for a, b in e2e_ev))
+    # per-stage device times (eager step with events between stages)
+    stages = {s: 0.0 for s in api.Fitter.STAGES}
+    reps = 5
+    for _ in range(reps):
+        flush.fill_(0.0)
+        for s, v in f.profile_step().items():
+            stages[s] += v / reps
+    cnt = f.counters()
+    code, flags = f.status()
+    f.close()
+    out = dict(t_ms=t_max, e2e_ms=e2e_ms, loss=loss, psnr=psnr_from_ref_loss(loss),
+               stages=stages, counters=cnt, clocks=clk.summary(), status=code, prob=prob)
+    return out
+
+
+def run_reference(args, world, rank, local):
+    import torch
+    from oracle import ref
+    from diffsplat_b200.scenes import reference_default
+
+    if not ref.available():
+        return None, "reference build oracle/_ref/libdsref.so is absent"
+    prob = reference_default(seed=rank)
+    R = ref.RefScene(prob.width, prob.height, prob.params, prob.sh_degree, prob.target, prob.pv,
+                     prob.cam, prob.lrs)
+    flush = torch.empty(FLUSH_BYTES // 4, device="cuda")
+    for _ in range(args.warmup):
+        R.step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            R.step()  # the reference runs on the legacy default stream
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    loss = R.loss()
+    R.close()
+    return dict(t_ms=t_ms, loss=loss, clocks=clk.summary()), None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup(args.gpus)
+    config = {"workload": "reference-default fitter: 1280x720 procedural target (2000 blobs), "
+                          "60000 splats, SH 0, 16x16 tiles, MSE, Adam (Gaussian3DAdamConfig lrs)",
+              "width": 1280, "height": 720, "splats": 60000, "sh_degree": 0,
+              "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"}
+    line = {"metric": METRIC, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural)",
+            "config": config}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        res, why = run_reference(args, 1, 0, local)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        v = args.steps / (res["t_ms"] / 1e3)
+        line.update({"impl": "reference", "n_gpus": 1, "value": v,
+                     "ms_per_step": res["t_ms"] / args.steps, "clocks": res["clocks"],
+                     "final_loss": res["loss"],
+                     "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0},
+                     "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1,
+                                      "kind": "reference",
+                                      "sample": "the reference's own CUDA layers (it has no CPU "
+                                                "path) built for sm_100a, driven by 1 host "
+                                                "thread; ImageFitter::step per step"}})
+        print(json.dumps(line))
+        return
+    r = run_ours(args, world, rank, local)
+    if rank != 0:
+        return
+    prob = r["prob"]
+    steps_total = world * args.steps
+    value = steps_total / (r["t_ms"] / 1e3)
+    pixels = prob.width * prob.height
+    tiles = ((prob.width + 15) // 16) * ((prob.height + 15) // 16)
+    isects = r["counters"]["n_isects"]
+    n = prob.params.shape[1]
+    sb = stage_bytes(n, isects, pixels, tiles)
+    stages = r["stages"]
+    dom = max(stages, key=stages.get)
+    peaks = measured_peaks()
+    achieved = sb[dom] / (stages[dom] * 1e-3) / 1e9
+    line.update({
+        "value": value, "ms_per_step": r["t_ms"] / args.steps,
+        "mpix_per_s": value * pixels / 1e6,
+        "e2e": {"value": steps_total / (r["e2e_ms"] / 1e3), "unit": "steps/s",
+                "h2d_bytes_per_step": 80, "d2h_bytes_per_step": 4},
+        "gpu_launches": kernels_per_step(tiles) * args.steps,
+        "clocks": r["clocks"],
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": None, "peak_src": peaks["src"],
+                     "algorithmic_bytes": sb[dom]},
+        "stage_ms": stages, "n_isects": isects, "visible": r["counters"]["visible"],
+        "final_loss": r["loss"], "status": r["status"],
+    })
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_oracle(prob)
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

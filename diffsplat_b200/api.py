@@ -1,0 +1,328 @@
+"""Python front end of the C ABI, operating on CUDA torch tensors.
+
+SoA tensors are field-major 2-D float32 tensors on the GPU:
+  Gaussian3D  [14 + 3K, n]  pos xyz, log-scale xyz, quat wxyz, sh_dc rgb, logit,
+                            sh_rest r (K rows), g (K rows), b (K rows)
+  Splat3D     [13, n]       pos xyz, cov xx xy xz yy yz zz, rgb, opacity
+  Splat2D     [10, n]       ndc xyz, cov xx xy yy, rgb, opacity
+(the row orders of the reference's SoA types, src/types/*.h, with the SH rest
+moved after the logit so the 14 scalar fields are contiguous).  Images are
+[H, W, 3] float32.  Torch provides device memory and the stream; every
+computation runs in libdiffsplat_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .scenes import sh_bands
+
+# row index of each Gaussian3D struct field in the [14 + 3K, n] layout
+_G3_ROWS = {"pos_x": 0, "pos_y": 1, "pos_z": 2, "scale_x": 3, "scale_y": 4, "scale_z": 5,
+            "rot_w": 6, "rot_x": 7, "rot_y": 8, "rot_z": 9, "sh_dc_r": 10, "sh_dc_g": 11,
+            "sh_dc_b": 12, "logit_opacity": 13}
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _check2d(t: torch.Tensor, rows: int | None = None) -> None:
+    if not (t.is_cuda and t.dtype == torch.float32 and t.dim() == 2 and t.is_contiguous()):
+        raise ValueError("expected a contiguous float32 CUDA tensor [rows, n]")
+    if rows is not None and t.shape[0] != rows:
+        raise ValueError(f"expected {rows} rows, got {t.shape[0]}")
+
+
+def g3_view(t: torch.Tensor, bands: int) -> L.Gaussian3D:
+    _check2d(t, 14 + 3 * bands)
+    n = t.shape[1]
+    base = t.data_ptr()
+    g = L.Gaussian3D()
+    for name, row in _G3_ROWS.items():
+        setattr(g, name, base + 4 * row * n)
+    if bands > 0:
+        g.sh_rest_r = base + 4 * 14 * n
+        g.sh_rest_g = base + 4 * (14 + bands) * n
+        g.sh_rest_b = base + 4 * (14 + 2 * bands) * n
+    g.count = n
+    g.sh_num_bands = bands
+    return g
+
+
+def g3_tensor_from_view(g: L.Gaussian3D) -> torch.Tensor:
+    """Wraps a contiguous Gaussian3D allocation (as laid out by ds_fitter) as a
+    [14 + 3K, n] tensor view without copying."""
+    n, K = g.count, g.sh_num_bands
+    rows = 14 + 3 * K
+    # ds_fitter carves pos..logit (14 rows) then rest r, g, b: same as _G3_ROWS except
+    # the logit row, which precedes the rest in both layouts.
+    ptr = g.pos_x
+    if g.logit_opacity != ptr + 4 * 13 * n:
+        raise ValueError("Gaussian3D view is not in the contiguous fitter layout")
+    return _wrap_device(ptr, (rows, n))
+
+
+def _wrap_device(ptr: int, shape) -> torch.Tensor:
+    numel = int(np.prod(shape))
+
+    class _Holder:
+        __cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": "<f4", "data": (ptr, False), "version": 3,
+            "strides": None}
+
+    return torch.as_tensor(_Holder(), device="cuda").view(*shape) if numel else torch.empty(
+        shape, device="cuda")
+
+
+def s3_view(t: torch.Tensor) -> L.Splat3D:
+    _check2d(t, 13)
+    n = t.shape[1]
+    s = L.Splat3D()
+    for k, name in enumerate(L.SPLAT3D_FIELDS):
+        setattr(s, name, t.data_ptr() + 4 * k * n)
+    s.count = n
+    return s
+
+
+def s2_view(t: torch.Tensor) -> L.Splat2D:
+    _check2d(t, 10)
+    n = t.shape[1]
+    s = L.Splat2D()
+    for k, name in enumerate(L.SPLAT2D_FIELDS):
+        setattr(s, name, t.data_ptr() + 4 * k * n)
+    s.count = n
+    return s
+
+
+# ---- GaussActivLayer ---------------------------------------------------------------
+def activ_forward(params: torch.Tensor, degree: int, cam_pos, out: torch.Tensor | None = None,
+                  stream=None) -> torch.Tensor:
+    bands = params.shape[0] - 14
+    if bands % 3:
+        raise ValueError("params rows must be 14 + 3K")
+    n = params.shape[1]
+    if out is None:
+        out = torch.zeros((13, n), device=params.device, dtype=torch.float32)
+    L.call("ds_activ_forward", C.byref(g3_view(params, bands // 3)), degree,
+           L.fptr(cam_pos), C.byref(s3_view(out)), _stream(stream))
+    return out
+
+
+def activ_backward(params, saved_out, grad_out, degree: int, cam_pos, grad_in=None, stream=None):
+    bands = (params.shape[0] - 14) // 3
+    if grad_in is None:
+        grad_in = torch.zeros_like(params)
+    L.call("ds_activ_backward", C.byref(g3_view(params, bands)), C.byref(s3_view(saved_out)),
+           C.byref(s3_view(grad_out)), degree, L.fptr(cam_pos), C.byref(g3_view(grad_in, bands)),
+           _stream(stream))
+    return grad_in
+
+
+# ---- PerspProjectLayer ---------------------------------------------------------------
+def project_forward(s3: torch.Tensor, pv, out: torch.Tensor | None = None, stream=None):
+    if out is None:
+        out = torch.zeros((10, s3.shape[1]), device=s3.device, dtype=torch.float32)
+    L.call("ds_project_forward", C.byref(s3_view(s3)), L.fptr(pv), C.byref(s2_view(out)),
+           _stream(stream))
+    return out
+
+
+def project_backward(s3: torch.Tensor, pv, grad_out: torch.Tensor, grad_in=None, stream=None,
+                     grad_mode: int = L.DS_GRAD_REFERENCE):
+    if grad_in is None:
+        grad_in = torch.zeros((13, s3.shape[1]), device=s3.device, dtype=torch.float32)
+    L.call("ds_project_backward_ex", C.byref(s3_view(s3)), L.fptr(pv),
+           C.byref(s2_view(grad_out)), C.byref(s3_view(grad_in)), grad_mode, _stream(stream))
+    return grad_in
+
+
+# ---- TileRasterizeLayer ----------------------------------------------------------------
+class Rasterizer:
+    """Owns a ds_raster handle (the reference's TileRasterizeLayer state)."""
+
+    def __init__(self, width: int, height: int, max_splats: int, max_isects: int = 0):
+        h = C.c_void_p()
+        L.call("ds_raster_create", width, height, max_splats, max_isects, C.byref(h))
+        self.h = h
+        self.width, self.height = width, height
+        self.tiles = ((width + 15) // 16) * ((height + 15) // 16)
+
+    def set_grad_mode(self, mode: int) -> None:
+        L.call("ds_raster_set_grad_mode", self.h, mode)
+
+    def close(self):
+        if self.h:
+            L.lib().ds_raster_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, s2: torch.Tensor, out: torch.Tensor | None = None, stream=None):
+        if out is None:
+            out = torch.empty((self.height, self.width, 3), device=s2.device, dtype=torch.float32)
+        L.call("ds_raster_forward", self.h, C.byref(s2_view(s2)), out.data_ptr(), _stream(stream))
+        return out
+
+    def backward(self, s2: torch.Tensor, grad_rgb: torch.Tensor, grad_in=None, stream=None):
+        if grad_in is None:
+            grad_in = torch.zeros_like(s2)
+        L.call("ds_raster_backward", self.h, C.byref(s2_view(s2)), grad_rgb.data_ptr(),
+               C.byref(s2_view(grad_in)), _stream(stream))
+        return grad_in
+
+    def visible_count(self) -> int:
+        v = C.c_uint32()
+        L.call("ds_raster_visible_count", self.h, C.byref(v))
+        return v.value
+
+    def isect_count(self) -> int:
+        v = C.c_uint32()
+        L.call("ds_raster_isect_count", self.h, C.byref(v))
+        return v.value
+
+    def status(self) -> tuple[int, int]:
+        v = C.c_uint32()
+        code = L.lib().ds_raster_status(self.h, C.byref(v))
+        return code, v.value
+
+    def download(self, what: int, n_splats: int = 0) -> np.ndarray:
+        n = min(self.isect_count(), 1 << 31)
+        px = self.width * self.height
+        spec = {L.DS_RASTER_KEYS: (np.uint64, n), L.DS_RASTER_IDS: (np.uint32, n),
+                L.DS_RASTER_RANGES: (np.int32, 2 * self.tiles),
+                L.DS_RASTER_LAST_IDS: (np.int32, px), L.DS_RASTER_ALPHAS: (np.float32, px),
+                L.DS_RASTER_COUNTS: (np.uint32, n_splats)}[what]
+        arr = np.zeros(max(spec[1], 1), spec[0])
+        L.call("ds_raster_download", self.h, what, arr.ctypes.data, arr.nbytes)
+        return arr[:spec[1]]
+
+
+# ---- MSELossLayer --------------------------------------------------------------------
+def mse_forward(pixels: torch.Tensor, target: torch.Tensor, stream=None) -> torch.Tensor:
+    loss = torch.empty(1, device=pixels.device, dtype=torch.float32)
+    L.call("ds_mse_forward", pixels.data_ptr(), target.data_ptr(), pixels.numel() // 3,
+           loss.data_ptr(), _stream(stream))
+    return loss
+
+
+def mse_backward(pixels: torch.Tensor, target: torch.Tensor, stream=None) -> torch.Tensor:
+    grad = torch.empty_like(pixels)
+    L.call("ds_mse_backward", pixels.data_ptr(), target.data_ptr(), pixels.numel() // 3,
+           grad.data_ptr(), _stream(stream))
+    return grad
+
+
+# ---- Adam --------------------------------------------------------------------------------
+def adam_step(groups, step: int, beta1=0.9, beta2=0.999, eps=1e-8, stream=None) -> None:
+    """groups: iterable of (param, grad, m, v, lr) float32 CUDA tensors."""
+    gs = list(groups)
+    arr = (L.AdamGroup * max(len(gs), 1))()
+    for k, (p, g, m, v, lr) in enumerate(gs):
+        arr[k] = L.AdamGroup(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(),
+                             float(lr))
+    L.call("ds_adam_step", arr, len(gs), beta1, beta2, eps, step, _stream(stream))
+
+
+# ---- fused fitter ----------------------------------------------------------------------
+class Fitter:
+    """Owns a ds_fitter (the graph-captured ImageFitter::step)."""
+
+    def __init__(self, width: int, height: int, count: int, sh_degree: int = 0, lrs=None,
+                 max_isects: int = 0, use_graph: bool = True, keep_grads: bool = False,
+                 storage: int = L.DS_STORAGE_FP32, betas=(0.9, 0.999), eps: float = 1e-8,
+                 grad_mode: int = L.DS_GRAD_REFERENCE):
+        cfg = L.FitterConfig()
+        L.call("ds_fitter_default_config", C.byref(cfg))
+        cfg.width, cfg.height, cfg.count, cfg.sh_degree = width, height, count, sh_degree
+        cfg.max_isects = max_isects
+        if lrs is not None:
+            (cfg.lr_pos, cfg.lr_scale, cfg.lr_rot, cfg.lr_sh_dc, cfg.lr_sh_rest,
+             cfg.lr_opacity) = lrs
+        cfg.beta1, cfg.beta2 = betas
+        cfg.epsilon = eps
+        cfg.storage = storage
+        cfg.use_graph = 1 if use_graph else 0
+        cfg.grad_mode = grad_mode
+        h = C.c_void_p()
+        L.call("ds_fitter_create_with_grads" if keep_grads else "ds_fitter_create", C.byref(cfg),
+               C.byref(h))
+        self.h = h
+        self.width, self.height, self.count, self.sh_degree = width, height, count, sh_degree
+        self.bands = sh_bands(sh_degree)
+        g = L.Gaussian3D()
+        L.call("ds_fitter_params", self.h, C.byref(g))
+        self.params = g3_tensor_from_view(g)
+        self.keep_grads = keep_grads
+
+    def close(self):
+        if self.h:
+            L.lib().ds_fitter_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params) -> None:
+        self.params.copy_(torch.as_tensor(params, device="cuda"))
+
+    def set_target(self, target: torch.Tensor, stream=None) -> None:
+        target = target.contiguous()
+        L.call("ds_fitter_set_target", self.h, target.data_ptr(), _stream(stream))
+        self._target = target
+
+    def set_camera(self, pv, cam_pos, stream=None) -> None:
+        L.call("ds_fitter_set_camera", self.h, L.fptr(pv), L.fptr(cam_pos), _stream(stream))
+
+    def step(self, n: int = 1, stream=None) -> None:
+        L.call("ds_fitter_step", self.h, n, _stream(stream))
+
+    def loss(self, stream=None) -> float:
+        v = C.c_float()
+        L.call("ds_fitter_loss", self.h, C.byref(v), _stream(stream))
+        return v.value
+
+    def image(self) -> torch.Tensor:
+        p = C.c_void_p()
+        L.call("ds_fitter_output", self.h, C.byref(p))
+        return _wrap_device(p.value, (self.height, self.width, 3))
+
+    def grads(self) -> torch.Tensor:
+        g = L.Gaussian3D()
+        L.call("ds_fitter_grads", self.h, C.byref(g))
+        return g3_tensor_from_view(g)
+
+    def moments(self):
+        m, v = L.Gaussian3D(), L.Gaussian3D()
+        L.call("ds_fitter_moments", self.h, C.byref(m), C.byref(v))
+        return g3_tensor_from_view(m), g3_tensor_from_view(v)
+
+    def status(self) -> tuple[int, int]:
+        v = C.c_uint32()
+        code = L.lib().ds_fitter_status(self.h, C.byref(v))
+        return code, v.value
+
+    STAGES = ("preprocess", "depth_sort", "scan_emit", "tile_sort_ranges", "composite_fwd",
+              "composite_bwd", "backward_adam")
+
+    def profile_step(self, stream=None) -> dict:
+        """One eager step with CUDA events between stages; returns ms per stage."""
+        ms = (C.c_float * 7)()
+        L.call("ds_fitter_profile_step", self.h, ms, 7, _stream(stream))
+        return dict(zip(self.STAGES, list(ms)))
+
+    def counters(self) -> dict:
+        out = (C.c_uint64 * 3)()
+        L.call("ds_fitter_counters", self.h, out, 3)
+        return {"n_isects": int(out[0]), "visible": int(out[1]), "step": int(out[2])}

@@ -1,0 +1,164 @@
+// Internal host-side declarations shared by the .cu files of libdiffsplat_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/diffsplat_b200.h"
+
+namespace ds {
+
+inline int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return DS_OK;
+  if (e == cudaErrorMemoryAllocation) return DS_ERR_OOM;
+  return DS_ERR_CUDA;
+}
+
+#define DS_TRY(expr)                 \
+  do {                               \
+    int _st = (expr);                \
+    if (_st != DS_OK) return _st;    \
+  } while (0)
+
+#define DS_CUDA(expr) DS_TRY(::ds::cuda_status(expr))
+
+// Layer kernels (ds_activ_project.cu)
+int launch_activ_forward(const ds_gaussian3d& in, int degree, const float cam[3],
+                         const ds_splat3d& out, cudaStream_t s);
+int launch_activ_backward(const ds_gaussian3d& in, const ds_splat3d& saved,
+                          const ds_splat3d& gout, int degree, const float cam[3],
+                          const ds_gaussian3d& gin, cudaStream_t s);
+int launch_project_forward(const ds_splat3d& in, const float pv[16], const ds_splat2d& out,
+                           cudaStream_t s);
+int launch_project_backward(const ds_splat3d& in, const float pv[16], const ds_splat2d& gout,
+                            const ds_splat3d& gin, int mode, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (uint32 key, uint32 value) pairs (ds_sort.cu).
+// The element count is read from device memory so the whole pipeline can be
+// captured into a CUDA graph.  Fixed grid of kSortBlocks CTAs.
+// ---------------------------------------------------------------------------
+constexpr int kSortBlocks = 296;    // 2 x 148 SMs
+constexpr int kSortTileItems = 2048;  // items per CTA iteration (8 warps x 32 lanes x 8)
+
+struct SortScratch {
+  uint32_t* hist = nullptr;  // [256 * kSortBlocks]
+};
+
+// Sorts n = min(*n_dev, cap) pairs by key bits [0, bits).  Pass 0 reads
+// (kin, vin) and writes (ka, va); later passes alternate (ka, va) <-> (kb, vb).
+// kb may alias kin (the input is consumed by pass 0); ka may not.  *out_k /
+// *out_v receive the buffers holding the result.  vin == nullptr means the
+// input values are 0..n-1.  When gather_src != nullptr, the last pass also
+// writes gather_dst[q] = gather_src[value[q]].
+int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uint32_t* va,
+                     uint32_t* kb, uint32_t* vb, uint32_t** out_k, uint32_t** out_v,
+                     const uint32_t* n_dev, uint32_t cap, int bits, const uint32_t* gather_src,
+                     uint32_t* gather_dst, SortScratch& scratch, cudaStream_t s);
+
+// Exclusive scan of counts gathered through a permutation:
+//   offsets[p] = sum_{q < p} counts[perm[q]]   (64-bit),
+//   *raw_total = the full sum, *n_clamped = min(raw_total, cap), and the
+//   overflow bit is or-ed into *status when raw_total > cap.
+struct ScanScratch {
+  unsigned long long* partials = nullptr;  // [kSortBlocks + 1]
+};
+int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
+                         unsigned long long* offsets, uint32_t* n_clamped,
+                         unsigned long long* raw_total, uint32_t cap, uint32_t* status,
+                         ScanScratch& scratch, cudaStream_t s);
+
+// Device-resident scalars of one rasterizer / fitter.
+struct DevScalars {
+  uint32_t n_isects;  // (tile, splat) pairs of the last forward, clamped to capacity
+  uint32_t visible;   // splats with a non-empty tile rectangle
+  uint32_t status;    // sticky StatusBits
+  uint32_t ticket;    // CTA-completion counter of the fused loss reduction
+  uint32_t n_splats;  // element count of the depth sort
+  uint32_t step;      // Adam step count (fitter)
+  uint32_t pad[2];
+  unsigned long long n_isects_raw;  // unclamped pair count
+  float loss;
+  float pad2[3];
+};
+
+// ---------------------------------------------------------------------------
+// Rasterizer state (ds_raster.cu), shared by the layer API and the fitter.
+// ---------------------------------------------------------------------------
+struct RasterBuffers {
+  int width = 0, height = 0, ntx = 0, nty = 0, tiles = 0;
+  int max_splats = 0;
+  int64_t cap = 0;  // intersection capacity
+  int grad_mode = DS_GRAD_REFERENCE;
+
+  // per splat
+  float4* rec_a = nullptr;
+  float4* rec_b = nullptr;
+  float4* rec_c = nullptr;
+  float* rec_idet = nullptr;
+  ushort4* rect = nullptr;     // tile rectangle {x0, x1, y0, y1}
+  uint32_t* counts = nullptr;  // tiles per splat (0 = invisible)
+  uint32_t* seg_start = nullptr;  // first emission index of each splat
+  uint32_t* depth_keys = nullptr;  // depth key of each splat (0xffffffff when invisible)
+  uint32_t* depth_k0 = nullptr;    // ping-pong buffers of the depth sort
+  uint32_t* depth_k1 = nullptr;
+  uint32_t* depth_v0 = nullptr;
+  uint32_t* depth_v1 = nullptr;
+  unsigned long long* emit_offsets = nullptr;  // exclusive scan of counts in depth order
+
+  // per intersection
+  uint32_t* tile_k0 = nullptr;
+  uint32_t* tile_k1 = nullptr;
+  uint32_t* tile_v0 = nullptr;
+  uint32_t* tile_v1 = nullptr;
+  uint32_t* emit_splat = nullptr;  // splat id of each emission slot
+  uint32_t* sorted_splat = nullptr;
+  float* isect_grad = nullptr;  // [cap * 9] per-(tile, splat) gradient partials
+
+  // results of the last sort (point into the ping-pong buffers)
+  uint32_t* sorted_tile = nullptr;
+  uint32_t* sorted_emit = nullptr;
+  uint32_t* depth_perm = nullptr;         // depth-sorted splat ids
+  uint32_t* depth_sorted_keys = nullptr;  // their depth keys
+
+  // per tile / pixel
+  int2* ranges = nullptr;
+  float* alphas = nullptr;
+  int32_t* last_ids = nullptr;
+  float* loss_partials = nullptr;  // [tiles]
+
+  DevScalars* scalars = nullptr;
+
+  SortScratch sort;
+  ScanScratch scan;
+};
+
+int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap);
+int raster_resize(RasterBuffers& rb, int width, int height);
+void raster_free(RasterBuffers& rb);
+
+// Everything after the per-splat records exist: depth sort, emission, tile
+// sort, ranges.  Records, rect, counts and depth_keys must be filled for n splats.
+int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev = nullptr);
+
+// Composite forward.  When target != nullptr the per-tile squared error is
+// also accumulated and reduced into rb.scalars->loss (L = sum / pixels).
+int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* target,
+                             cudaStream_t s);
+// Composite backward into rb.isect_grad.  dL/dpixel is read from grad_rgb, or,
+// when grad_rgb == nullptr, computed as 2/P (image - target).
+int raster_composite_backward(RasterBuffers& rb, const float* image, const float* grad_rgb,
+                              const float* target, cudaStream_t s);
+
+// Layer-API preprocess from Splat2D SoA, and reduction of isect_grad into Splat2D grads.
+int raster_prepare_from_splat2d(RasterBuffers& rb, const ds_splat2d& in, cudaStream_t s);
+int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStream_t s);
+
+// Losses and Adam (ds_loss_adam.cu)
+int launch_mse_forward(const float* px, const float* tgt, int64_t npix, float* loss,
+                       float* partials, uint32_t* ticket, cudaStream_t s);
+int launch_mse_backward(const float* px, const float* tgt, int64_t npix, float* grad,
+                        cudaStream_t s);
+int launch_adam_multi(const ds_adam_group* groups, int n_groups, float beta1, float beta2,
+                      float eps, float bc1, float bc2, cudaStream_t s);
+
+}  // namespace ds

@@ -1,0 +1,295 @@
+// Stable LSD radix sort of (uint32 key, uint32 value) pairs and the exclusive
+// scan that turns per-splat tile counts into emission offsets.
+//
+// This replaces the reference's cub::DeviceRadixSort::SortPairs over all 64
+// key bits (src/layers/tile_rasterize_layer.cu:664-684).  The rasterizer sorts
+// in two stages instead (depth keys of the splats, then tile ids of the
+// emitted pairs, see ds_raster.cu), and each stage only sorts the bits it
+// needs.  Element counts are read from device memory and every launch has a
+// fixed grid, so the sort runs inside a captured CUDA graph without the
+// reference's host read of n_isects (:660-661).
+//
+// Per pass (8-bit digit), three kernels:
+//   hist    : per-CTA digit histogram of its contiguous chunk -> hist[digit][cta]
+//   scan    : one CTA turns the digit-major histogram into exclusive offsets
+//   scatter : each CTA re-reads its chunk 2048 items at a time, ranks items
+//             stably inside each warp with __match_any_sync, combines warp
+//             counts in shared memory and writes every item to its slot.
+#include "ds_common.cuh"
+#include "ds_internal.h"
+
+namespace ds {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = kSortTileItems / kThreads;  // 8 per lane
+
+__device__ __forceinline__ uint32_t sort_chunk(uint32_t n) {
+  uint32_t per = (n + kSortBlocks - 1) / kSortBlocks;
+  return (per + kSortTileItems - 1) / kSortTileItems * kSortTileItems;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    radix_hist_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ n_dev,
+                      uint32_t cap, int shift, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[256];
+  const uint32_t n = min(*n_dev, cap);
+  const uint32_t chunk = sort_chunk(n);
+  const uint32_t begin = min(blockIdx.x * chunk, n);
+  const uint32_t end = min(begin + chunk, n);
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  // Warp-aggregated shared-memory counting: one atomic per distinct digit per warp.
+  for (uint32_t base = begin; base < end; base += kThreads) {
+    uint32_t i = base + threadIdx.x;
+    uint32_t d = i < end ? ((keys[i] >> shift) & 255u) : 0x100u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  hist[threadIdx.x * kSortBlocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of `total` entries with one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) scan_hist_kernel(uint32_t* __restrict__ hist, int total) {
+  __shared__ uint32_t warp_tot[32];
+  const int per = (total + 1023) / 1024;
+  const int begin = min((int)threadIdx.x * per, total);
+  const int end = min(begin + per, total);
+  uint32_t s = 0;
+  for (int i = begin; i < end; ++i) s += hist[i];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t x = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    warp_tot[lane] = x;  // inclusive
+  }
+  __syncthreads();
+  uint32_t excl = incl - s + (w > 0 ? warp_tot[w - 1] : 0u);
+  for (int i = begin; i < end; ++i) {
+    uint32_t v = hist[i];
+    hist[i] = excl;
+    excl += v;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    radix_scatter_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                         int iota, uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                         const uint32_t* __restrict__ n_dev, uint32_t cap, int shift,
+                         const uint32_t* __restrict__ offs, const uint32_t* __restrict__ gsrc,
+                         uint32_t* __restrict__ gdst) {
+  __shared__ uint32_t cnt[kWarps][256];
+  __shared__ uint32_t base[256];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t n = min(*n_dev, cap);
+  const uint32_t chunk = sort_chunk(n);
+  const uint32_t begin = min(blockIdx.x * chunk, n);
+  const uint32_t end = min(begin + chunk, n);
+  if (begin >= end) return;
+  base[threadIdx.x] = offs[threadIdx.x * kSortBlocks + blockIdx.x];
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t t0 = begin; t0 < end; t0 += kSortTileItems) {
+    for (int d = lane; d < 256; d += 32) cnt[w][d] = 0;
+    __syncwarp();
+    uint32_t key[kItems], val[kItems], rank[kItems];
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      bool ok = idx < end;
+      key[it] = ok ? kin[idx] : 0u;
+      val[it] = ok ? (iota ? idx : vin[idx]) : 0u;
+    }
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      bool ok = idx < end;
+      uint32_t d = ok ? ((key[it] >> shift) & 255u) : 0x100u;
+      uint32_t peers = __match_any_sync(0xffffffffu, d);
+      uint32_t pre = ok ? cnt[w][d] : 0u;
+      __syncwarp();
+      if (ok && lane == __ffs(peers) - 1) cnt[w][d] = pre + __popc(peers);
+      __syncwarp();
+      rank[it] = pre + __popc(peers & lt);
+    }
+    __syncthreads();
+    {
+      uint32_t run = base[threadIdx.x];
+#pragma unroll
+      for (int ww = 0; ww < kWarps; ++ww) {
+        uint32_t c = cnt[ww][threadIdx.x];
+        cnt[ww][threadIdx.x] = run;
+        run += c;
+      }
+      base[threadIdx.x] = run;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      if (idx < end) {
+        uint32_t d = (key[it] >> shift) & 255u;
+        uint32_t dst = cnt[w][d] + rank[it];
+        kout[dst] = key[it];
+        vout[dst] = val[it];
+        if (gdst) gdst[dst] = gsrc[val[it]];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- permuted exclusive scan of counts -----------------------------------
+constexpr int kScanItems = 4;
+
+__device__ __forceinline__ uint32_t scan_chunk(uint32_t n) {
+  uint32_t per = (n + kSortBlocks - 1) / kSortBlocks;
+  const uint32_t step = kThreads * kScanItems;
+  return (per + step - 1) / step * step;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    scan_partial_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
+                        uint32_t n, unsigned long long* __restrict__ partials) {
+  __shared__ unsigned long long wsum[kWarps];
+  const uint32_t chunk = scan_chunk(n);
+  const uint32_t begin = min(blockIdx.x * chunk, n);
+  const uint32_t end = min(begin + chunk, n);
+  unsigned long long s = 0;
+  for (uint32_t p = begin + threadIdx.x; p < end; p += kThreads) s += counts[perm[p]];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int k = 0; k < kWarps; ++k) t += wsum[k];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    scan_partials_kernel(unsigned long long* __restrict__ partials, uint32_t cap,
+                         uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
+                         uint32_t* __restrict__ status) {
+  __shared__ unsigned long long buf[kSortBlocks];
+  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) buf[i] = partials[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (int i = 0; i < kSortBlocks; ++i) {
+      unsigned long long v = buf[i];
+      buf[i] = run;
+      run += v;
+    }
+    *raw = run;
+    *n_clamped = (uint32_t)(run < (unsigned long long)cap ? run : cap);
+    if (run > (unsigned long long)cap) atomicOr(status, kStatusIsectOverflow);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) partials[i] = buf[i];
+}
+
+__global__ void __launch_bounds__(kThreads)
+    scan_final_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
+                      uint32_t n, const unsigned long long* __restrict__ partials,
+                      unsigned long long* __restrict__ offsets) {
+  __shared__ unsigned long long wsum[kWarps];
+  const uint32_t chunk = scan_chunk(n);
+  const uint32_t begin = min(blockIdx.x * chunk, n);
+  const uint32_t end = min(begin + chunk, n);
+  if (begin >= end) return;
+  unsigned long long carry = partials[blockIdx.x];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t t0 = begin; t0 < end; t0 += kThreads * kScanItems) {
+    uint32_t c[kScanItems];
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      uint32_t p = t0 + threadIdx.x * kScanItems + k;
+      c[k] = p < end ? counts[perm[p]] : 0u;
+      s += c[k];
+    }
+    unsigned long long incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    unsigned long long wbase = 0, tot = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) {
+      unsigned long long v = wsum[k];
+      if (k < w) wbase += v;
+      tot += v;
+    }
+    unsigned long long excl = carry + wbase + incl - s;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      uint32_t p = t0 + threadIdx.x * kScanItems + k;
+      if (p < end) offsets[p] = excl;
+      excl += c[k];
+    }
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uint32_t* va,
+                     uint32_t* kb, uint32_t* vb, uint32_t** out_k, uint32_t** out_v,
+                     const uint32_t* n_dev, uint32_t cap, int bits, const uint32_t* gather_src,
+                     uint32_t* gather_dst, SortScratch& scratch, cudaStream_t s) {
+  const int passes = bits <= 0 ? 1 : (bits + 7) / 8;
+  const uint32_t* src_k = kin;
+  const uint32_t* src_v = vin;
+  uint32_t* dst_k = ka;
+  uint32_t* dst_v = va;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    const bool last = p == passes - 1;
+    radix_hist_kernel<<<kSortBlocks, kThreads, 0, s>>>(src_k, n_dev, cap, shift, scratch.hist);
+    scan_hist_kernel<<<1, 1024, 0, s>>>(scratch.hist, 256 * kSortBlocks);
+    radix_scatter_kernel<<<kSortBlocks, kThreads, 0, s>>>(
+        src_k, src_v, src_v == nullptr ? 1 : 0, dst_k, dst_v, n_dev, cap, shift, scratch.hist,
+        last ? gather_src : nullptr, last ? gather_dst : nullptr);
+    *out_k = dst_k;
+    *out_v = dst_v;
+    src_k = dst_k;
+    src_v = dst_v;
+    dst_k = (dst_k == ka) ? kb : ka;
+    dst_v = (dst_v == va) ? vb : va;
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
+                         unsigned long long* offsets, uint32_t* n_clamped,
+                         unsigned long long* raw_total, uint32_t cap, uint32_t* status,
+                         ScanScratch& scratch, cudaStream_t s) {
+  scan_partial_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials);
+  scan_partials_kernel<<<1, kThreads, 0, s>>>(scratch.partials, cap, n_clamped, raw_total,
+                                              status);
+  scan_final_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, offsets);
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace ds

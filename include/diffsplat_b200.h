@@ -1,0 +1,239 @@
+/*
+ * diffsplat_b200 -- C ABI of the B200 (sm_100a) differentiable Gaussian-splatting
+ * training path.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream (as
+ * void*), and returns an int status (DS_OK == 0).  Calls that launch work are
+ * stream-ordered and asynchronous unless their comment says they synchronise.
+ * Buffers passed in are owned by the caller; opaque handles (ds_raster,
+ * ds_fitter) own the scratch they allocate and free it in *_destroy.
+ *
+ * Struct field order and array layouts are those of the reference's SoA types,
+ * so a caller holding reference buffers can pass them unchanged:
+ *   ds_gaussian3d  <->  Gaussian3DParams / Gaussian3DGrads (src/types/gaussian3d.h:34-120)
+ *   ds_splat3d     <->  Splat3DParams / Splat3DGrads       (src/types/splat3d.h:14-51)
+ *   ds_splat2d     <->  Splat2DParams / Splat2DGrads       (src/types/splat2d.h:13-45)
+ * Higher-order SH buffers are band-major: sh_rest_r[band * count + i].
+ * Images are interleaved RGB float [H*W*3], row-major, top row first.
+ */
+#ifndef DIFFSPLAT_B200_H
+#define DIFFSPLAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DS_ABI_VERSION 1
+
+/* Status codes. */
+#define DS_OK 0
+#define DS_ERR_ARG 1            /* invalid argument (null pointer, bad size, bad degree) */
+#define DS_ERR_OOM 2            /* device allocation failed */
+#define DS_ERR_CUDA 3           /* a CUDA runtime call or kernel launch failed */
+#define DS_ERR_ISECT_OVERFLOW 4 /* more (tile, splat) pairs than the intersection buffer holds */
+#define DS_ERR_STATE 5          /* call made in the wrong state (e.g. step before set_target) */
+#define DS_ERR_NO_DEVICE 6      /* no CUDA device, or not an sm_100 device */
+
+/* Storage modes for ds_fitter. */
+#define DS_STORAGE_FP32 0 /* all attributes, SH and Adam moments in FP32 */
+#define DS_STORAGE_BF16 1 /* attributes, SH and Adam moments in BF16; FP32 master weights */
+
+/* Gradient of the compositing backward with respect to alpha.
+ * DS_GRAD_REFERENCE reproduces the reference's recurrence
+ * (src/layers/tile_rasterize_layer.cu:518-521), which weighs the colour of the
+ * splats behind by T_before instead of dividing it by T_after; it is the true
+ * derivative only when no later splat contributes.  DS_GRAD_EXACT is the true
+ * derivative (matches finite differences). */
+#define DS_GRAD_REFERENCE 0
+#define DS_GRAD_EXACT 1
+
+typedef void *ds_stream; /* cudaStream_t; NULL selects the legacy default stream */
+
+typedef struct ds_gaussian3d {
+  float *pos_x, *pos_y, *pos_z;
+  float *scale_x, *scale_y, *scale_z;       /* log-scale */
+  float *rot_w, *rot_x, *rot_y, *rot_z;     /* raw quaternion, normalised in kernel */
+  float *sh_dc_r, *sh_dc_g, *sh_dc_b;
+  float *sh_rest_r, *sh_rest_g, *sh_rest_b; /* [band*count + i]; NULL when sh_num_bands == 0 */
+  float *logit_opacity;
+  int32_t count;
+  int32_t sh_num_bands; /* 0, 3, 8 or 15 */
+} ds_gaussian3d;
+
+typedef struct ds_splat3d {
+  float *pos_x, *pos_y, *pos_z;
+  float *cov_xx, *cov_xy, *cov_xz;
+  float *cov_yy, *cov_yz, *cov_zz;
+  float *color_r, *color_g, *color_b;
+  float *opacity;
+  int32_t count;
+} ds_splat3d;
+
+typedef struct ds_splat2d {
+  float *pos_x, *pos_y, *pos_z;    /* NDC */
+  float *cov_xx, *cov_xy, *cov_yy; /* NDC units */
+  float *color_r, *color_g, *color_b;
+  float *opacity;
+  int32_t count;
+} ds_splat2d;
+
+/* Library information. */
+int ds_abi_version(void);
+const char *ds_status_string(int status);
+/* Returns DS_OK when a device of compute capability 10.x is present. */
+int ds_device_check(void);
+
+/* ---- Activation: replaces GaussActivLayer::forward / ::backward
+ *      (src/layers/gauss_activ_layer.cu:411-440, :442-476; kernels :37-170, :198-407).
+ *      cam_pos is the host array setCameraPosition() stores
+ *      (src/layers/gauss_activ_layer.h:33). */
+int ds_activ_forward(const ds_gaussian3d *in, int sh_degree, const float cam_pos[3],
+                     const ds_splat3d *out, ds_stream stream);
+/* Writes (does not accumulate) grad_in; reads the saved forward output `out`
+ * for the clamp and sigmoid gates, like the reference. */
+int ds_activ_backward(const ds_gaussian3d *in, const ds_splat3d *out, const ds_splat3d *grad_out,
+                      int sh_degree, const float cam_pos[3], const ds_gaussian3d *grad_in,
+                      ds_stream stream);
+
+/* ---- Projection: replaces PerspProjectLayer::forward / ::backward / ::setCamera
+ *      (src/layers/persp_project_layer.cu:316-334, :336-355, :307-312).
+ *      pv is the column-major 16-float PV = proj * view that setCamera uploads;
+ *      here it is passed per call, so two layers may use different cameras. */
+int ds_project_forward(const ds_splat3d *in, const float pv[16], const ds_splat2d *out,
+                       ds_stream stream);
+int ds_project_backward(const ds_splat3d *in, const float pv[16], const ds_splat2d *grad_out,
+                        const ds_splat3d *grad_in, ds_stream stream);
+/* Same with a gradient mode: DS_GRAD_EXACT also carries the position
+ * dependence of the Jacobian (hence of Cov2D) into dL/dpos, which the
+ * reference's backward (persp_project_layer.cu:245-260) leaves out. */
+int ds_project_backward_ex(const ds_splat3d *in, const float pv[16], const ds_splat2d *grad_out,
+                           const ds_splat3d *grad_in, int grad_mode, ds_stream stream);
+
+/* ---- Tile rasterizer: replaces TileRasterizeLayer (src/layers/tile_rasterize_layer.h:23-60,
+ *      .cu:591-617 allocate, :619-633 resize, :637-708 forward, :710-728 backward,
+ *      :582-587 getVisibleCount).  The handle owns the intersection buffers. */
+typedef struct ds_raster ds_raster;
+
+/* max_isects <= 0 selects the reference's 2^25 pairs. */
+int ds_raster_create(int width, int height, int max_splats, int64_t max_isects, ds_raster **out);
+int ds_raster_resize(ds_raster *r, int width, int height);
+/* DS_GRAD_REFERENCE (default) or DS_GRAD_EXACT for the following backward calls. */
+int ds_raster_set_grad_mode(ds_raster *r, int mode);
+/* Forward: tile keys, sort, ranges and front-to-back compositing into out_rgb
+ * [H*W*3] (overwritten, background black).  Asynchronous: no host sync. */
+int ds_raster_forward(ds_raster *r, const ds_splat2d *in, float *out_rgb, ds_stream stream);
+/* Backward of the last forward.  ACCUMULATES into grad_in (like the reference's
+ * atomicAdd into zeroed buffers), deterministically. */
+int ds_raster_backward(ds_raster *r, const ds_splat2d *in, const float *grad_rgb,
+                       const ds_splat2d *grad_in, ds_stream stream);
+/* Number of splats with a non-empty tile rectangle in the last forward (synchronises). */
+int ds_raster_visible_count(ds_raster *r, uint32_t *out);
+/* Number of (tile, splat) pairs of the last forward, before clamping to capacity (synchronises). */
+int ds_raster_isect_count(ds_raster *r, uint32_t *out);
+/* Reads and clears the sticky status bits (synchronises).  Returns
+ * DS_ERR_ISECT_OVERFLOW when a forward since the last call overflowed. */
+int ds_raster_status(ds_raster *r, uint32_t *flags);
+/* Copies internal state of the last forward to host memory (synchronises):
+ *   DS_RASTER_KEYS      uint64 [n_isects]  sorted (tile_id << 32 | depth bits) keys
+ *   DS_RASTER_IDS       uint32 [n_isects]  sorted splat ids (ascending id within equal keys)
+ *   DS_RASTER_RANGES    int32  [2*tiles]   per-tile {start, end}; {0,0} for empty tiles
+ *   DS_RASTER_LAST_IDS  int32  [H*W]       sorted-list index of each pixel's last contributor
+ *   DS_RASTER_ALPHAS    float  [H*W]       1 - final transmittance
+ *   DS_RASTER_COUNTS    uint32 [count]     tiles covered per splat */
+#define DS_RASTER_KEYS 0
+#define DS_RASTER_IDS 1
+#define DS_RASTER_RANGES 2
+#define DS_RASTER_LAST_IDS 3
+#define DS_RASTER_ALPHAS 4
+#define DS_RASTER_COUNTS 5
+int ds_raster_download(ds_raster *r, int what, void *host, int64_t bytes);
+int ds_raster_destroy(ds_raster *r);
+
+/* ---- Loss: replaces MSELossLayer::forward / ::backward / ::getLoss
+ *      (src/layers/mse_loss_layer.cu:85-92, :94-99, :101-105).
+ *      L = sum_px sum_c (r - t)^2 / num_pixels  (normalised by pixels, not pixels*3).
+ *      ds_mse_forward overwrites *loss (device scalar). */
+int ds_mse_forward(const float *pixels, const float *target, int64_t num_pixels, float *loss,
+                   ds_stream stream);
+int ds_mse_backward(const float *pixels, const float *target, int64_t num_pixels, float *grad,
+                    ds_stream stream);
+
+/* ---- Adam: replaces Adam::step (src/optimizers/adam.cu:59-73, kernel :12-37).
+ *      All groups are updated by ONE launch.  `step` is the 1-based step count
+ *      after increment; bias corrections are computed on the host exactly as
+ *      the reference does (1 / (1 - powf(beta, step))). */
+typedef struct ds_adam_group {
+  float *param;
+  const float *grad;
+  float *m;
+  float *v;
+  int64_t n;
+  float lr;
+} ds_adam_group;
+int ds_adam_step(const ds_adam_group *groups, int n_groups, float beta1, float beta2,
+                 float epsilon, int step, ds_stream stream);
+
+/* ---- Fused fitter: one training step of ImageFitter::step
+ *      (src/pipelines/image_fitter.cpp:103-112: zeroGrad, forward, backward, Adam)
+ *      with the layers of src/pipelines/image_fitter.cpp:63-101 fused into a
+ *      fixed sequence of kernels that is captured once into a CUDA graph.
+ *      Learning rates default to Gaussian3DAdamConfig (src/optimizers/gaussian3d_adam.h:11-19). */
+typedef struct ds_fitter ds_fitter;
+
+typedef struct ds_fitter_config {
+  int32_t width, height;
+  int32_t count;      /* splats */
+  int32_t sh_degree;  /* 0..3 */
+  int64_t max_isects; /* <= 0: 2^25 */
+  float lr_pos, lr_scale, lr_rot, lr_sh_dc, lr_sh_rest, lr_opacity;
+  float beta1, beta2, epsilon;
+  int32_t storage;   /* DS_STORAGE_FP32 / DS_STORAGE_BF16 */
+  int32_t use_graph; /* 1: capture the step into a CUDA graph on first use */
+  int32_t grad_mode; /* DS_GRAD_REFERENCE (default) / DS_GRAD_EXACT */
+} ds_fitter_config;
+
+int ds_fitter_default_config(ds_fitter_config *cfg);
+int ds_fitter_create(const ds_fitter_config *cfg, ds_fitter **out);
+/* Device views of the fitter's FP32 master parameters (write them before the first step). */
+int ds_fitter_params(ds_fitter *f, ds_gaussian3d *out);
+/* Copies the target image [H*W*3] from a device pointer. */
+int ds_fitter_set_target(ds_fitter *f, const float *target, ds_stream stream);
+/* Camera for the following steps (column-major PV and world camera position, host arrays). */
+int ds_fitter_set_camera(ds_fitter *f, const float pv[16], const float cam_pos[3],
+                         ds_stream stream);
+/* Runs n_steps training steps (asynchronous). */
+int ds_fitter_step(ds_fitter *f, int n_steps, ds_stream stream);
+/* Loss of the most recent step's forward (synchronises the stream). */
+int ds_fitter_loss(ds_fitter *f, float *loss, ds_stream stream);
+/* Device pointer of the rendered image [H*W*3] of the most recent forward. */
+int ds_fitter_output(ds_fitter *f, float **image);
+int ds_fitter_step_count(ds_fitter *f, int *out);
+/* Reads and clears sticky status bits (synchronises). */
+int ds_fitter_status(ds_fitter *f, uint32_t *flags);
+int ds_fitter_destroy(ds_fitter *f);
+
+/* Inspection hooks of the fused fitter (no reference counterpart: the
+ * reference exposes its gradients through GaussActivLayer::getGradInput,
+ * src/layers/layer.h:59).  A fitter made by ds_fitter_create_with_grads also
+ * writes each step's Gaussian3D gradients, readable through ds_fitter_grads;
+ * ds_fitter_moments returns device views of the Adam first/second moments. */
+int ds_fitter_create_with_grads(const ds_fitter_config *cfg, ds_fitter **out);
+/* One step run eagerly with CUDA events between its stages (synchronises);
+ * stage_ms[0..6] = preprocess, depth sort, scan + emission, tile sort + ranges,
+ * composite forward, composite backward, backward + Adam.  It advances the
+ * optimizer like ds_fitter_step. */
+int ds_fitter_profile_step(ds_fitter *f, float *stage_ms, int n_stages, ds_stream stream);
+/* out[0] = (tile, splat) pairs, out[1] = visible splats, out[2] = device step
+ * count, all of the most recent step (synchronises). */
+int ds_fitter_counters(ds_fitter *f, uint64_t *out, int n);
+int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
+int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* DIFFSPLAT_B200_H */
