@@ -240,6 +240,28 @@ def run_reference(args, world, rank, local):
     return dict(t_ms=t_ms, loss=loss, clocks=clk.summary()), None
 
 
+def profile_run(args):
+    """Eager (non-graph) steps of the bench workload for profilers: every kernel
+    is a separate launch, device memory stays under 1 GB."""
+    import torch
+    from diffsplat_b200 import api
+    from diffsplat_b200.scenes import reference_default
+    torch.cuda.set_device(0)
+    prob = reference_default(seed=0)
+    f = api.Fitter(prob.width, prob.height, prob.params.shape[1], prob.sh_degree, lrs=prob.lrs,
+                   max_isects=1 << 22, use_graph=False)
+    f.set_params(prob.params)
+    f.set_target(torch.tensor(prob.target, device="cuda"))
+    f.set_camera(prob.pv, prob.cam)
+    f.step(args.warmup + args.steps)
+    torch.cuda.synchronize()
+    code, flags = f.status()
+    print(f"profile run: {args.warmup + args.steps} steps, loss {f.loss():.6f}, status {code}")
+    f.close()
+    if code != 0:
+        sys.exit(1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,7 +269,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="untimed: warmup + steps eager steps of the same workload with a "
+                         "2^22-pair buffer (for ncu captures); prints no JSON line")
     args = ap.parse_args()
+    if args.profile_run:
+        profile_run(args)
+        return
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args.gpus)
     config = {"workload": "reference-default fitter: 1280x720 procedural target (2000 blobs), "

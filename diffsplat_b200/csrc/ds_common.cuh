@@ -55,8 +55,14 @@ struct UnitQuat {
   float inv_norm;
 };
 
+// Rounding of the sums on the tile-key path is pinned with explicit
+// fma/mul/add intrinsics: nvcc's choice of which product to fuse depends on the
+// surrounding code, and the forms below are the ones that reproduce the
+// reference build's FP32 results bit for bit (measured against it on the GPU
+// over 10^5 random splats with a general camera).
 __device__ __forceinline__ UnitQuat unit_quat(float w, float x, float y, float z) {
-  float inv = rsqrtf(fmaxf(w * w + x * x + y * y + z * z, 1e-12f));
+  float n2 = __fmaf_rn(z, z, __fmaf_rn(y, y, __fmaf_rn(w, w, __fmul_rn(x, x))));
+  float inv = rsqrtf(fmaxf(n2, 1e-12f));
   return {w * inv, x * inv, y * inv, z * inv, inv};
 }
 
@@ -64,18 +70,29 @@ struct Rot3 {
   float r00, r01, r02, r10, r11, r12, r20, r21, r22;
 };
 
+// R = I + 2 [ -(y^2+z^2)  xy-wz  xz+wy ; xy+wz  -(x^2+z^2)  yz-wx ; xz-wy  yz+wx  -(x^2+y^2) ]
 __device__ __forceinline__ Rot3 rot_from_quat(float qw, float qx, float qy, float qz) {
   Rot3 R;
-  R.r00 = 1.f - 2.f * (qy * qy + qz * qz);
-  R.r01 = 2.f * (qx * qy - qw * qz);
-  R.r02 = 2.f * (qx * qz + qw * qy);
-  R.r10 = 2.f * (qx * qy + qw * qz);
-  R.r11 = 1.f - 2.f * (qx * qx + qz * qz);
-  R.r12 = 2.f * (qy * qz - qw * qx);
-  R.r20 = 2.f * (qx * qz - qw * qy);
-  R.r21 = 2.f * (qy * qz + qw * qx);
-  R.r22 = 1.f - 2.f * (qx * qx + qy * qy);
+  R.r00 = 1.f - 2.f * __fadd_rn(__fmul_rn(qy, qy), __fmul_rn(qz, qz));
+  R.r01 = 2.f * __fmaf_rn(qx, qy, -__fmul_rn(qw, qz));
+  R.r02 = 2.f * __fmaf_rn(qx, qz, __fmul_rn(qw, qy));
+  R.r10 = 2.f * __fmaf_rn(qx, qy, __fmul_rn(qw, qz));
+  R.r11 = 1.f - 2.f * __fmaf_rn(qx, qx, __fmul_rn(qz, qz));
+  R.r12 = 2.f * __fmaf_rn(qy, qz, -__fmul_rn(qw, qx));
+  R.r20 = 2.f * __fmaf_rn(qx, qz, -__fmul_rn(qw, qy));
+  R.r21 = 2.f * __fmaf_rn(qy, qz, __fmul_rn(qw, qx));
+  R.r22 = 1.f - 2.f * __fmaf_rn(qx, qx, __fmul_rn(qy, qy));
   return R;
+}
+
+// a0 b0 + a1 b1 + a2 b2 with the first product fused (A) or the second (B).
+__device__ __forceinline__ float dot3_a(float a0, float b0, float a1, float b1, float a2,
+                                        float b2) {
+  return __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, __fmul_rn(a0, b0)));
+}
+__device__ __forceinline__ float dot3_b(float a0, float b0, float a1, float b1, float a2,
+                                        float b2) {
+  return __fmaf_rn(a2, b2, __fmaf_rn(a0, b0, __fmul_rn(a1, b1)));
 }
 
 __device__ __forceinline__ float3 dir_to_camera(float cx, float cy, float cz, float px, float py,
@@ -95,12 +112,12 @@ __device__ __forceinline__ Cov3 cov3_from(const Rot3& R, float sx, float sy, flo
   float m10 = R.r10 * sx, m11 = R.r11 * sy, m12 = R.r12 * sz;
   float m20 = R.r20 * sx, m21 = R.r21 * sy, m22 = R.r22 * sz;
   Cov3 c;
-  c.xx = m00 * m00 + m01 * m01 + m02 * m02;
-  c.xy = m00 * m10 + m01 * m11 + m02 * m12;
-  c.xz = m00 * m20 + m01 * m21 + m02 * m22;
-  c.yy = m10 * m10 + m11 * m11 + m12 * m12;
-  c.yz = m10 * m20 + m11 * m21 + m12 * m22;
-  c.zz = m20 * m20 + m21 * m21 + m22 * m22;
+  c.xx = dot3_a(m00, m00, m01, m01, m02, m02);
+  c.xy = dot3_b(m00, m10, m01, m11, m02, m12);
+  c.xz = dot3_a(m00, m20, m01, m21, m02, m22);
+  c.yy = dot3_b(m10, m10, m11, m11, m12, m12);
+  c.yz = dot3_b(m10, m20, m11, m21, m12, m22);
+  c.zz = dot3_b(m20, m20, m21, m21, m22, m22);
   return c;
 }
 
@@ -186,10 +203,10 @@ struct Proj2 {
 __device__ __forceinline__ void project_jacobian(const Mat4& P, float x, float y, float z,
                                                  float& clip_x, float& clip_y, float& clip_z,
                                                  float& clip_w) {
-  clip_x = P.m[0] * x + P.m[4] * y + P.m[8] * z + P.m[12];
-  clip_y = P.m[1] * x + P.m[5] * y + P.m[9] * z + P.m[13];
-  clip_z = P.m[2] * x + P.m[6] * y + P.m[10] * z + P.m[14];
-  clip_w = P.m[3] * x + P.m[7] * y + P.m[11] * z + P.m[15];
+  clip_x = __fadd_rn(dot3_a(P.m[4], y, P.m[0], x, P.m[8], z), P.m[12]);
+  clip_y = __fadd_rn(dot3_a(P.m[5], y, P.m[1], x, P.m[9], z), P.m[13]);
+  clip_z = __fadd_rn(dot3_a(P.m[6], y, P.m[2], x, P.m[10], z), P.m[14]);
+  clip_w = __fadd_rn(dot3_a(P.m[7], y, P.m[3], x, P.m[11], z), P.m[15]);
 }
 
 struct Jac2 {
@@ -199,12 +216,12 @@ struct Jac2 {
 __device__ __forceinline__ Jac2 jacobian(const Mat4& P, float clip_x, float clip_y, float clip_w,
                                          float inv_w2) {
   Jac2 J;
-  J.j00 = (P.m[0] * clip_w - clip_x * P.m[3]) * inv_w2;
-  J.j01 = (P.m[4] * clip_w - clip_x * P.m[7]) * inv_w2;
-  J.j02 = (P.m[8] * clip_w - clip_x * P.m[11]) * inv_w2;
-  J.j10 = (P.m[1] * clip_w - clip_y * P.m[3]) * inv_w2;
-  J.j11 = (P.m[5] * clip_w - clip_y * P.m[7]) * inv_w2;
-  J.j12 = (P.m[9] * clip_w - clip_y * P.m[11]) * inv_w2;
+  J.j00 = __fmaf_rn(P.m[0], clip_w, -__fmul_rn(clip_x, P.m[3])) * inv_w2;
+  J.j01 = __fmaf_rn(P.m[4], clip_w, -__fmul_rn(clip_x, P.m[7])) * inv_w2;
+  J.j02 = __fmaf_rn(P.m[8], clip_w, -__fmul_rn(clip_x, P.m[11])) * inv_w2;
+  J.j10 = __fmaf_rn(P.m[1], clip_w, -__fmul_rn(clip_y, P.m[3])) * inv_w2;
+  J.j11 = __fmaf_rn(P.m[5], clip_w, -__fmul_rn(clip_y, P.m[7])) * inv_w2;
+  J.j12 = __fmaf_rn(P.m[9], clip_w, -__fmul_rn(clip_y, P.m[11])) * inv_w2;
   return J;
 }
 
@@ -215,16 +232,16 @@ struct Cov2 {
 // Cov2D = J Cov3D J^T, upper triangle (persp_project_layer.cu:164-180).
 __device__ __forceinline__ Cov2 cov2_from(const Jac2& J, float cxx, float cxy, float cxz, float cyy,
                                           float cyz, float czz) {
-  float js00 = J.j00 * cxx + J.j01 * cxy + J.j02 * cxz;
-  float js01 = J.j00 * cxy + J.j01 * cyy + J.j02 * cyz;
-  float js02 = J.j00 * cxz + J.j01 * cyz + J.j02 * czz;
-  float js10 = J.j10 * cxx + J.j11 * cxy + J.j12 * cxz;
-  float js11 = J.j10 * cxy + J.j11 * cyy + J.j12 * cyz;
-  float js12 = J.j10 * cxz + J.j11 * cyz + J.j12 * czz;
+  float js00 = dot3_b(J.j00, cxx, J.j01, cxy, J.j02, cxz);
+  float js01 = dot3_b(J.j00, cxy, J.j01, cyy, J.j02, cyz);
+  float js02 = dot3_b(J.j00, cxz, J.j01, cyz, J.j02, czz);
+  float js10 = dot3_b(J.j10, cxx, J.j11, cxy, J.j12, cxz);
+  float js11 = dot3_b(J.j10, cxy, J.j11, cyy, J.j12, cyz);
+  float js12 = dot3_b(J.j10, cxz, J.j11, cyz, J.j12, czz);
   Cov2 c;
-  c.xx = J.j00 * js00 + J.j01 * js01 + J.j02 * js02;
-  c.xy = J.j00 * js10 + J.j01 * js11 + J.j02 * js12;
-  c.yy = J.j10 * js10 + J.j11 * js11 + J.j12 * js12;
+  c.xx = dot3_b(J.j00, js00, J.j01, js01, J.j02, js02);
+  c.xy = dot3_b(J.j00, js10, J.j01, js11, J.j02, js12);
+  c.yy = dot3_b(J.j10, js10, J.j11, js11, J.j12, js12);
   return c;
 }
 
@@ -236,10 +253,20 @@ struct TileRect {
   int x0, x1, y0, y1;
 };
 
+// det of Cov2D and the conic's quadratic form dx^2 a + 2 dx dy b + dy^2 c, in
+// the reference's rounding (tile_rasterize_layer.cu:150, :321, :341).
+__device__ __forceinline__ float conic_det(float cxx, float cxy, float cyy) {
+  return __fmaf_rn(cxx, cyy, -__fmul_rn(cxy, cxy));
+}
+__device__ __forceinline__ float conic_dist2(float dx, float dy, float a, float b, float c) {
+  const float t2 = __fmul_rn(__fmul_rn(2.f, dx), dy);
+  return __fmaf_rn(__fmul_rn(dy, dy), c, __fmaf_rn(__fmul_rn(dx, dx), a, __fmul_rn(t2, b)));
+}
+
 __device__ __forceinline__ bool tile_rect(float x, float y, float z, float cxx, float cxy, float cyy,
                                           int width, int height, int ntx, int nty, TileRect& r) {
   if (!(fabsf(x) <= 1.0f && fabsf(y) <= 1.0f && fabsf(z) <= 1.0f)) return false;
-  float det = cxx * cyy - cxy * cxy;
+  float det = conic_det(cxx, cxy, cyy);
   if (!(det > 0.f)) return false;
   float extent_x = 3.f * sqrtf(cxx);
   float extent_y = 3.f * sqrtf(cyy);
@@ -283,7 +310,7 @@ struct Record {
 __device__ __forceinline__ Record make_record(float x, float y, float cxx, float cxy, float cyy,
                                               float r, float g, float b, float opac) {
   Record rec;
-  float det = cxx * cyy - cxy * cxy;
+  float det = conic_det(cxx, cxy, cyy);
   float idet = 1.f / det;
   float icxx = cyy * idet;
   float icxy = -cxy * idet;

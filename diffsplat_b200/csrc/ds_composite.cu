@@ -1,0 +1,417 @@
+// Front-to-back compositing of one 16x16 tile per CTA and its backward.
+//
+// Semantics: src/layers/tile_rasterize_layer.cu:192-309 (forward) and
+// :356-578 (backward): NDC pixel centres, conic from Cov2D, sigma < 0 skip,
+// alpha = min(0.99, o exp(-sigma)), alpha < 1/255 skip, termination after
+// including the splat that brings T to <= 1e-4, last_ids = sorted-list index of
+// the last contributor, backward by reverse traversal with
+// T_before = T / max(1 - alpha, 1e-6).
+//
+// Layout: each thread owns PPT pixels of one column (PPT = 1, 2 or 4); a warp
+// covers a BW x BH block (8x4, 8x8 or 16x8 pixels) and tests each splat's
+// conservative acceptance box against that block once, so the shared-memory
+// reads, the culling test and (backward) the warp reduction are shared by
+// 32 * PPT pixels.  The backward keeps one gradient partial per warp and splat
+// in shared memory and sums the warps in a fixed order: gradients are
+// deterministic run to run.
+#include <stdlib.h>
+
+#include "ds_common.cuh"
+#include "ds_internal.h"
+
+namespace ds {
+
+namespace {
+
+constexpr int kFwdBatch = 256;  // splats staged in shared memory per forward batch
+
+template <int PPT>
+struct Lay {
+  static constexpr int kThreads = kTilePixels / PPT;
+  static constexpr int kWarps = kThreads / 32;
+  static constexpr int BW = PPT == 4 ? 16 : 8;  // warp block width
+  static constexpr int BH = 32 * PPT / BW;      // warp block height
+  static constexpr int kLaneRows = 32 / BW;     // rows between a thread's pixels
+  static constexpr int kWarpsX = kTile / BW;
+  static constexpr int kBwdBatch = 64 * PPT;    // keeps the per-warp partials at 18 KB
+};
+
+template <int PPT>
+struct Pixels {
+  int j;       // column
+  int i[PPT];  // rows
+  bool inside[PPT];
+  float px;
+  float py[PPT];
+  float wx_lo, wx_hi, wy_lo, wy_hi;  // extremes of the warp's pixel centres (NDC)
+};
+
+template <int PPT>
+__device__ __forceinline__ Pixels<PPT> pixels(int tile, int ntx, int W, int H) {
+  using Lc = Lay<PPT>;
+  Pixels<PPT> m;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int trow = tile / ntx, tcol = tile - trow * ntx;
+  const int lx = lane % Lc::BW, ly = lane / Lc::BW;
+  const int wx = w % Lc::kWarpsX, wy = w / Lc::kWarpsX;
+  m.j = tcol * kTile + wx * Lc::BW + lx;
+  m.px = 2.f * (m.j + 0.5f) / W - 1.f;
+  float yl = 3.0e38f, yh = -3.0e38f;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    m.i[k] = trow * kTile + wy * Lc::BH + ly + k * Lc::kLaneRows;
+    m.inside[k] = m.i[k] < H && m.j < W;
+    m.py[k] = 1.f - 2.f * (m.i[k] + 0.5f) / H;
+    yl = fminf(yl, m.py[k]);
+    yh = fmaxf(yh, m.py[k]);
+  }
+  float xl = m.px, xh = m.px;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    xl = fminf(xl, __shfl_xor_sync(0xffffffffu, xl, o));
+    xh = fmaxf(xh, __shfl_xor_sync(0xffffffffu, xh, o));
+    yl = fminf(yl, __shfl_xor_sync(0xffffffffu, yl, o));
+    yh = fmaxf(yh, __shfl_xor_sync(0xffffffffu, yh, o));
+  }
+  m.wx_lo = xl;
+  m.wx_hi = xh;
+  m.wy_lo = yl;
+  m.wy_hi = yh;
+  return m;
+}
+
+template <int PPT>
+__device__ __forceinline__ bool misses(const float4& a, const Pixels<PPT>& m) {
+  return a.x + a.z < m.wx_lo || a.x - a.z > m.wx_hi || a.y + a.w < m.wy_lo ||
+         a.y - a.w > m.wy_hi;
+}
+
+template <int PPT, bool kLoss>
+__global__ void __launch_bounds__(Lay<PPT>::kThreads)
+    composite_fwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
+                         const float4* __restrict__ rc, const uint32_t* __restrict__ sorted_splat,
+                         const int2* __restrict__ ranges, float* __restrict__ out_rgb,
+                         float* __restrict__ out_alpha, int32_t* __restrict__ last_ids, int W,
+                         int H, int ntx, const float* __restrict__ target,
+                         float* __restrict__ loss_partials, DevScalars* __restrict__ sc) {
+  using Lc = Lay<PPT>;
+  constexpr int NT = Lc::kThreads;
+  __shared__ float4 sA[kFwdBatch], sB[kFwdBatch], sC[kFwdBatch];
+  __shared__ float red[Lc::kWarps];
+  __shared__ bool last;
+  const int tile = blockIdx.x;
+  const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
+  const int2 range = ranges[tile];
+  const int start = range.x, end = range.y;
+  float T[PPT], Cr[PPT], Cg[PPT], Cb[PPT];
+  uint32_t cur[PPT];
+  bool done[PPT];
+  bool all_done = true;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    T[k] = 1.f;
+    Cr[k] = Cg[k] = Cb[k] = 0.f;
+    cur[k] = 0;
+    done[k] = !m.inside[k];
+    all_done = all_done && done[k];
+  }
+  for (int b0 = start; b0 < end; b0 += kFwdBatch) {
+    if (__syncthreads_count(all_done) >= NT) break;
+    for (int l = threadIdx.x; l < kFwdBatch; l += NT) {
+      const int idx = b0 + l;
+      if (idx < end) {
+        const uint32_t g = sorted_splat[idx];
+        sA[l] = ra[g];
+        sB[l] = rb[g];
+        sC[l] = rc[g];
+      }
+    }
+    __syncthreads();
+    const int bs = min(kFwdBatch, end - b0);
+    if (__any_sync(0xffffffffu, !all_done)) {
+      for (int t = 0; t < bs; ++t) {
+        const float4 a = sA[t];
+        if (misses<PPT>(a, m)) continue;
+        const float4 b = sB[t];
+        const float4 c = sC[t];
+        const float dx = a.x - m.px;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+          if (done[k]) continue;
+          const float dy = a.y - m.py[k];
+          const float sigma = 0.5f * conic_dist2(dx, dy, b.x, b.y, b.z);
+          if (sigma < 0.f || sigma > c.w) continue;
+          const float alpha = fminf(kMaxAlpha, b.w * __expf(-sigma));
+          if (alpha < kAlphaThres) continue;
+          const float vis = alpha * T[k];
+          Cr[k] = __fmaf_rn(c.x, vis, Cr[k]);
+          Cg[k] = __fmaf_rn(c.y, vis, Cg[k]);
+          Cb[k] = __fmaf_rn(c.z, vis, Cb[k]);
+          cur[k] = (uint32_t)(b0 + t);
+          T[k] = T[k] * (1.f - alpha);
+          if (T[k] <= kTThres) done[k] = true;
+        }
+        all_done = true;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) all_done = all_done && done[k];
+        if (!__any_sync(0xffffffffu, !all_done)) break;
+      }
+    }
+  }
+  float l = 0.f;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    if (!m.inside[k]) continue;
+    const int pix = m.i[k] * W + m.j;
+    out_rgb[pix * 3 + 0] = Cr[k];
+    out_rgb[pix * 3 + 1] = Cg[k];
+    out_rgb[pix * 3 + 2] = Cb[k];
+    out_alpha[pix] = 1.f - T[k];
+    last_ids[pix] = (int32_t)cur[k];
+    if (kLoss) {
+      const float scale = 1.f / (float)(W * H);
+      const float dR = Cr[k] - target[pix * 3 + 0];
+      const float dG = Cg[k] - target[pix * 3 + 1];
+      const float dB = Cb[k] - target[pix * 3 + 2];
+      l += (dR * dR + dG * dG + dB * dB) * scale;
+    }
+  }
+  if (kLoss) {
+    l = warp_sum(l);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float s = 0.f;
+      for (int k = 0; k < Lc::kWarps; ++k) s += red[k];
+      loss_partials[tile] = s;
+      __threadfence();
+      last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+      // The last CTA to finish sums the per-tile partials in tile order.
+      __threadfence();
+      float s = 0.f;
+      for (int k = threadIdx.x; k < (int)gridDim.x; k += NT)
+        s += ((volatile float*)loss_partials)[k];
+      s = warp_sum(s);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        float tot = 0.f;
+        for (int k = 0; k < Lc::kWarps; ++k) tot += red[k];
+        sc->loss = tot;
+        sc->ticket = 0u;
+      }
+    }
+  }
+}
+
+template <int PPT, bool kFusedLoss, bool kExact>
+__global__ void __launch_bounds__(Lay<PPT>::kThreads)
+    composite_bwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
+                         const float4* __restrict__ rc, const float* __restrict__ ridet,
+                         const uint32_t* __restrict__ sorted_splat,
+                         const uint32_t* __restrict__ sorted_emit, const int2* __restrict__ ranges,
+                         const float* __restrict__ alphas, const int32_t* __restrict__ last_ids,
+                         const float* __restrict__ grad_or_image, const float* __restrict__ target,
+                         float* __restrict__ isect_grad, int W, int H, int ntx) {
+  using Lc = Lay<PPT>;
+  constexpr int NT = Lc::kThreads;
+  constexpr int NW = Lc::kWarps;
+  constexpr int B = Lc::kBwdBatch;
+  __shared__ float4 sA[B], sB[B], sC[B];
+  __shared__ float sI[B];
+  __shared__ __align__(16) float part[NW][B * 9];  // per-warp partial of each batch splat
+  const int tile = blockIdx.x;
+  const int2 range = ranges[tile];
+  const int start = range.x, end = range.y;
+  if (end <= start) return;
+  const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float T[PPT], gr[PPT], gg[PPT], gb[PPT], accr[PPT], accg[PPT], accb[PPT];
+  int32_t fin[PPT];
+  int32_t my_final = -1;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    const int pix = min(m.i[k] * W + m.j, W * H - 1);
+    T[k] = 1.f - alphas[pix];
+    fin[k] = m.inside[k] ? last_ids[pix] : -1;
+    my_final = max(my_final, fin[k]);
+    gr[k] = gg[k] = gb[k] = 0.f;
+    if (m.inside[k]) {
+      if (kFusedLoss) {
+        const float scale = 2.f / (float)(W * H);
+        gr[k] = scale * (grad_or_image[pix * 3 + 0] - target[pix * 3 + 0]);
+        gg[k] = scale * (grad_or_image[pix * 3 + 1] - target[pix * 3 + 1]);
+        gb[k] = scale * (grad_or_image[pix * 3 + 2] - target[pix * 3 + 2]);
+      } else {
+        gr[k] = grad_or_image[pix * 3 + 0];
+        gg[k] = grad_or_image[pix * 3 + 1];
+        gb[k] = grad_or_image[pix * 3 + 2];
+      }
+    }
+    accr[k] = accg[k] = accb[k] = 0.f;
+  }
+  const int32_t warp_final = warp_max(my_final);
+  const int nb = (end - start + B - 1) / B;
+  for (int bi = 0; bi < nb; ++bi) {
+    const int batch_end = end - 1 - B * bi;  // farthest splat of the batch
+    const int bs = min(B, batch_end + 1 - start);
+    __syncthreads();
+    // stage the batch back to front: slot l holds sorted index batch_end - l
+    for (int l = threadIdx.x; l < B; l += NT) {
+      const int li = batch_end - l;
+      if (li >= start) {
+        const uint32_t g = sorted_splat[li];
+        sA[l] = ra[g];
+        sB[l] = rb[g];
+        sC[l] = rc[g];
+        sI[l] = ridet[g];
+      }
+    }
+    {
+      float4* p4 = reinterpret_cast<float4*>(&part[0][0]);
+      for (int q = threadIdx.x; q < NW * B * 9 / 4; q += NT) p4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    const int t_start = max(0, batch_end - warp_final);
+    for (int t = t_start; t < bs; ++t) {
+      const float4 a = sA[t];
+      if (misses<PPT>(a, m)) continue;
+      const float4 b = sB[t];
+      const float4 c = sC[t];
+      const float idet = sI[t];
+      const float dx = a.x - m.px;
+      const int sidx = batch_end - t;
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float va = 0.f;
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        if (!(m.inside[k] && sidx <= fin[k])) continue;
+        const float dy = a.y - m.py[k];
+        const float dist2 = conic_dist2(dx, dy, b.x, b.y, b.z);
+        const float sigma = 0.5f * dist2;
+        if (sigma < 0.f || sigma > c.w) continue;
+        const float opac = b.w;
+        const float g_exp = __expf(-sigma);
+        const float alpha = fminf(kMaxAlpha, opac * g_exp);
+        if (alpha < kAlphaThres) continue;
+        any = true;
+        const float T_before = T[k] / fmaxf(1.f - alpha, 1e-6f);
+        const float fac = alpha * T_before;
+        v[0] += fac * gr[k];
+        v[1] += fac * gg[k];
+        v[2] += fac * gb[k];
+        // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
+        // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
+        // exact derivative divides it by T_after instead.
+        const float ia = kExact ? 1.f / T[k] : 1.f;
+        const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
+                                          (c.y - accg[k] * ia) * gg[k] +
+                                          (c.z - accb[k] * ia) * gb[k]);
+        if (opac * g_exp <= kMaxAlpha) {
+          va += g_exp * v_alpha;
+          const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
+          const float ddx = 2.f * (dx * b.x + dy * b.y);
+          const float ddy = 2.f * (dx * b.y + dy * b.z);
+          v[3] += v_dist2 * ddx;
+          v[4] += v_dist2 * ddy;
+          v[5] += v_dist2 * (-0.25f * ddx * ddx);
+          v[7] += v_dist2 * (-0.25f * ddy * ddy);
+          v[6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * idet);
+        }
+        accr[k] += c.x * fac;
+        accg[k] += c.y * fac;
+        accb[k] += c.z * fac;
+        T[k] = T_before;
+      }
+      if (!__any_sync(0xffffffffu, any)) continue;
+      // lane 4q ends up with the warp sum of v[q]
+      const float s8 = warp_sum8_transposed(v, lane);
+      const float sa = warp_sum(va);
+      if ((lane & 3) == 0) part[w][t * 9 + (lane >> 2)] = s8;
+      if (lane == 0) part[w][t * 9 + 8] = sa;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < bs; l += NT) {
+      const uint32_t e = sorted_emit[batch_end - l];
+      float* dst = isect_grad + (size_t)e * 9;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        float s = 0.f;
+#pragma unroll
+        for (int ww = 0; ww < NW; ++ww) s += part[ww][l * 9 + q];
+        dst[q] = s;
+      }
+    }
+  }
+}
+
+template <int PPT>
+void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, cudaStream_t s) {
+  constexpr int NT = Lay<PPT>::kThreads;
+  if (target)
+    composite_fwd_kernel<PPT, true><<<rb.tiles, NT, 0, s>>>(
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, out_rgb, rb.alphas,
+        rb.last_ids, rb.width, rb.height, rb.ntx, target, rb.loss_partials, rb.scalars);
+  else
+    composite_fwd_kernel<PPT, false><<<rb.tiles, NT, 0, s>>>(
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, out_rgb, rb.alphas,
+        rb.last_ids, rb.width, rb.height, rb.ntx, nullptr, nullptr, rb.scalars);
+}
+
+template <int PPT>
+void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, const float* target,
+                cudaStream_t s) {
+  constexpr int NT = Lay<PPT>::kThreads;
+  const float* g = grad_rgb ? grad_rgb : image;
+  const float* t = grad_rgb ? nullptr : target;
+  const bool exact = rb.grad_mode == DS_GRAD_EXACT;
+#define DS_BWD(F, E)                                                                         \
+  composite_bwd_kernel<PPT, F, E><<<rb.tiles, NT, 0, s>>>(                                   \
+      rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit, rb.ranges, \
+      rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx)
+  if (grad_rgb) {
+    if (exact) DS_BWD(false, true);
+    else DS_BWD(false, false);
+  } else {
+    if (exact) DS_BWD(true, true);
+    else DS_BWD(true, false);
+  }
+#undef DS_BWD
+}
+
+}  // namespace
+
+int composite_default_ppt() {
+  const char* e = getenv("DS_COMPOSITE_PPT");
+  if (e) {
+    int v = atoi(e);
+    if (v == 1 || v == 2 || v == 4) return v;
+  }
+  return 1;
+}
+
+int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* target,
+                             cudaStream_t s) {
+  switch (rb.ppt) {
+    case 4: launch_fwd<4>(rb, out_rgb, target, s); break;
+    case 2: launch_fwd<2>(rb, out_rgb, target, s); break;
+    default: launch_fwd<1>(rb, out_rgb, target, s); break;
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+int raster_composite_backward(RasterBuffers& rb, const float* image, const float* grad_rgb,
+                              const float* target, cudaStream_t s) {
+  switch (rb.ppt) {
+    case 4: launch_bwd<4>(rb, image, grad_rgb, target, s); break;
+    case 2: launch_bwd<2>(rb, image, grad_rgb, target, s); break;
+    default: launch_bwd<1>(rb, image, grad_rgb, target, s); break;
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace ds

@@ -189,9 +189,7 @@ __device__ __forceinline__ void cov_backward(float rw, float rx, float ry, float
 __global__ void __launch_bounds__(kThreads)
     fit_backward_adam_kernel(ds_gaussian3d P, ds_gaussian3d M, ds_gaussian3d V, ds_gaussian3d G,
                              int keep_grads, int exact, int degree, const Camera* __restrict__ camp,
-                             const float* __restrict__ isect_grad,
-                             const uint32_t* __restrict__ seg_start,
-                             const uint32_t* __restrict__ counts, uint32_t cap,
+                             const float* __restrict__ g2sum,
                              const float2* __restrict__ bcp, Lrs lr, AdamHyper h) {
   __shared__ Mat4 sP;
   __shared__ float sCam[3];
@@ -203,19 +201,10 @@ __global__ void __launch_bounds__(kThreads)
   if (i >= n) return;
   const float2 bc = *bcp;
 
-  // 1) Splat2D gradient = sum of this splat's per-tile records.
-  float g2[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const uint32_t c = counts[i];
-  if (c) {
-    unsigned long long s = seg_start[i];
-    unsigned long long e = s + c;
-    if (e > cap) e = cap;
-    for (unsigned long long q = s; q < e; ++q) {
-      const float* r = isect_grad + q * 9;
+  // 1) Splat2D gradient = sum of this splat's per-tile records (segment_reduce_kernel).
+  float g2[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) g2[k] += r[k];
-    }
-  }
+  for (int k = 0; k < 9; ++k) g2[k] = g2sum[(size_t)k * n + i];
   // g2 = {color r, g, b, ndc x, ndc y, cov2 xx, xy, yy, opacity}
 
   // 2) projection backward (persp_project_layer.cu:245-305)
@@ -403,12 +392,13 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   if (ev) DS_CUDA(cudaEventRecord(ev[5], s));
   DS_TRY(raster_composite_backward(rb, f->image, nullptr, f->target, s));
   if (ev) DS_CUDA(cudaEventRecord(ev[6], s));
+  DS_TRY(raster_reduce_grads_soa(rb, n, s));
   Lrs lr{f->cfg.lr_pos, f->cfg.lr_scale, f->cfg.lr_rot, f->cfg.lr_sh_dc, f->cfg.lr_sh_rest,
          f->cfg.lr_opacity};
   AdamHyper h{f->cfg.beta1, f->cfg.beta2, f->cfg.epsilon};
   fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
-      f->P, f->M, f->V, f->G, f->g_mem ? 1 : 0, f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0, f->cfg.sh_degree, f->cam_dev, rb.isect_grad,
-      rb.seg_start, rb.counts, (uint32_t)rb.cap, f->bc_cur, lr, h);
+      f->P, f->M, f->V, f->G, f->g_mem ? 1 : 0, f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0,
+      f->cfg.sh_degree, f->cam_dev, rb.g2, f->bc_cur, lr, h);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[7], s));
   return DS_OK;

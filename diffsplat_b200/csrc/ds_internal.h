@@ -89,6 +89,7 @@ struct RasterBuffers {
   int max_splats = 0;
   int64_t cap = 0;  // intersection capacity
   int grad_mode = DS_GRAD_REFERENCE;
+  int ppt = 1;  // pixels per thread of the composite kernels (1, 2 or 4)
 
   // per splat
   float4* rec_a = nullptr;
@@ -104,6 +105,7 @@ struct RasterBuffers {
   uint32_t* depth_v0 = nullptr;
   uint32_t* depth_v1 = nullptr;
   unsigned long long* emit_offsets = nullptr;  // exclusive scan of counts in depth order
+  float* g2 = nullptr;  // [9][max_splats] per-splat Splat2D gradient sums (fitter path)
 
   // per intersection
   uint32_t* tile_k0 = nullptr;
@@ -133,6 +135,9 @@ struct RasterBuffers {
 };
 
 int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap);
+// Pixels per thread of the composite kernels; DS_COMPOSITE_PPT=1|2|4 overrides
+// the default (a tuning knob: results are identical for every value).
+int composite_default_ppt();
 int raster_resize(RasterBuffers& rb, int width, int height);
 void raster_free(RasterBuffers& rb);
 
@@ -152,6 +157,8 @@ int raster_composite_backward(RasterBuffers& rb, const float* image, const float
 // Layer-API preprocess from Splat2D SoA, and reduction of isect_grad into Splat2D grads.
 int raster_prepare_from_splat2d(RasterBuffers& rb, const ds_splat2d& in, cudaStream_t s);
 int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStream_t s);
+// Same sums written (not accumulated) to rb.g2 [9][n].
+int raster_reduce_grads_soa(RasterBuffers& rb, int n, cudaStream_t s);
 
 // Losses and Adam (ds_loss_adam.cu)
 int launch_mse_forward(const float* px, const float* tgt, int64_t npix, float* loss,

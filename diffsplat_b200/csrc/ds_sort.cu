@@ -26,8 +26,9 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kItems = kSortTileItems / kThreads;  // 8 per lane
 
-__device__ __forceinline__ uint32_t sort_chunk(uint32_t n) {
-  uint32_t per = (n + kSortBlocks - 1) / kSortBlocks;
+// Items per CTA: n split over G CTAs, rounded up to whole 2048-item tiles.
+__device__ __forceinline__ uint32_t sort_chunk(uint32_t n, uint32_t G) {
+  uint32_t per = (n + G - 1) / G;
   return (per + kSortTileItems - 1) / kSortTileItems * kSortTileItems;
 }
 
@@ -35,8 +36,9 @@ __global__ void __launch_bounds__(kThreads)
     radix_hist_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ n_dev,
                       uint32_t cap, int shift, uint32_t* __restrict__ hist) {
   __shared__ uint32_t h[256];
+  const uint32_t G = gridDim.x;
   const uint32_t n = min(*n_dev, cap);
-  const uint32_t chunk = sort_chunk(n);
+  const uint32_t chunk = sort_chunk(n, G);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   h[threadIdx.x] = 0;
@@ -50,41 +52,59 @@ __global__ void __launch_bounds__(kThreads)
     if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
   }
   __syncthreads();
-  hist[threadIdx.x * kSortBlocks + blockIdx.x] = h[threadIdx.x];
+  hist[threadIdx.x * G + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of `total` entries with one CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) scan_hist_kernel(uint32_t* __restrict__ hist, int total) {
-  __shared__ uint32_t warp_tot[32];
-  const int per = (total + 1023) / 1024;
-  const int begin = min((int)threadIdx.x * per, total);
-  const int end = min(begin + per, total);
-  uint32_t s = 0;
-  for (int i = begin; i < end; ++i) s += hist[i];
+// Exclusive scan of the digit-major histogram hist[digit * G + cta] with one
+// CTA of 1024 threads: warp w scans the G counts of digits w, w+32, ... in
+// coalesced 32-wide steps, then the 256 digit totals are scanned and added.
+__global__ void __launch_bounds__(1024) scan_hist_kernel(uint32_t* __restrict__ hist, int G) {
+  __shared__ uint32_t tot[256];
+  __shared__ uint32_t base[256];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  uint32_t incl = s;
+  for (int d = w; d < 256; d += 32) {
+    uint32_t* row = hist + (size_t)d * G;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < G; b0 += 32) {
+      const int b = b0 + lane;
+      const uint32_t v = b < G ? row[b] : 0u;
+      uint32_t incl = v;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (b < G) row[b] = carry + incl - v;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) tot[d] = carry;
   }
-  if (lane == 31) warp_tot[w] = incl;
   __syncthreads();
   if (w == 0) {
-    uint32_t x = warp_tot[lane];
+    uint32_t v[8], s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      v[k] = tot[lane * 8 + k];
+      s += v[k];
+    }
+    uint32_t incl = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += t;
+      uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
     }
-    warp_tot[lane] = x;  // inclusive
+    uint32_t run = incl - s;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      base[lane * 8 + k] = run;
+      run += v[k];
+    }
   }
   __syncthreads();
-  uint32_t excl = incl - s + (w > 0 ? warp_tot[w - 1] : 0u);
-  for (int i = begin; i < end; ++i) {
-    uint32_t v = hist[i];
-    hist[i] = excl;
-    excl += v;
+  for (int d = w; d < 256; d += 32) {
+    uint32_t* row = hist + (size_t)d * G;
+    const uint32_t add = base[d];
+    for (int b = lane; b < G; b += 32) row[b] += add;
   }
 }
 
@@ -98,11 +118,11 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint32_t base[256];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t n = min(*n_dev, cap);
-  const uint32_t chunk = sort_chunk(n);
+  const uint32_t chunk = sort_chunk(n, gridDim.x);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
-  base[threadIdx.x] = offs[threadIdx.x * kSortBlocks + blockIdx.x];
+  base[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x];
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t t0 = begin; t0 < end; t0 += kSortTileItems) {
     for (int d = lane; d < 256; d += 32) cnt[w][d] = 0;
@@ -259,6 +279,9 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
                      const uint32_t* n_dev, uint32_t cap, int bits, const uint32_t* gather_src,
                      uint32_t* gather_dst, SortScratch& scratch, cudaStream_t s) {
   const int passes = bits <= 0 ? 1 : (bits + 7) / 8;
+  // One CTA per 2048-item tile of the capacity, at most kSortBlocks.
+  const uint64_t tiles = ((uint64_t)cap + kSortTileItems - 1) / kSortTileItems;
+  const int G = (int)(tiles < 1 ? 1 : (tiles > (uint64_t)kSortBlocks ? kSortBlocks : tiles));
   const uint32_t* src_k = kin;
   const uint32_t* src_v = vin;
   uint32_t* dst_k = ka;
@@ -266,9 +289,9 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     const bool last = p == passes - 1;
-    radix_hist_kernel<<<kSortBlocks, kThreads, 0, s>>>(src_k, n_dev, cap, shift, scratch.hist);
-    scan_hist_kernel<<<1, 1024, 0, s>>>(scratch.hist, 256 * kSortBlocks);
-    radix_scatter_kernel<<<kSortBlocks, kThreads, 0, s>>>(
+    radix_hist_kernel<<<G, kThreads, 0, s>>>(src_k, n_dev, cap, shift, scratch.hist);
+    scan_hist_kernel<<<1, 1024, 0, s>>>(scratch.hist, G);
+    radix_scatter_kernel<<<G, kThreads, 0, s>>>(
         src_k, src_v, src_v == nullptr ? 1 : 0, dst_k, dst_v, n_dev, cap, shift, scratch.hist,
         last ? gather_src : nullptr, last ? gather_dst : nullptr);
     *out_k = dst_k;
