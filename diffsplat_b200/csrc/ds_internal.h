@@ -89,7 +89,7 @@ struct RasterBuffers {
   int max_splats = 0;
   int64_t cap = 0;  // intersection capacity
   int grad_mode = DS_GRAD_REFERENCE;
-  int ppt = 1;  // pixels per thread of the composite kernels (1, 2 or 4)
+  int ppt = 2;  // pixels per thread of the composite kernels (1, 2 or 4)
 
   // per splat
   float4* rec_a = nullptr;
