@@ -98,6 +98,7 @@ _SIGS = {
     "ds_raster_status": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
     "ds_raster_download": (C.c_int, [_vp, C.c_int, _vp, C.c_int64]),
     "ds_raster_destroy": (C.c_int, [_vp]),
+    "ds_raster_forward_noalloc": (C.c_int, [C.POINTER(Splat2D), C.c_int, C.c_int, _vp, _vp]),
     "ds_mse_forward": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp]),
     "ds_mse_backward": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp]),
     "ds_adam_step": (C.c_int, [C.POINTER(AdamGroup), C.c_int, C.c_float, C.c_float, C.c_float,

@@ -152,6 +152,21 @@ int ds_raster_status(ds_raster *r, uint32_t *flags);
 int ds_raster_download(ds_raster *r, int what, void *host, int64_t bytes);
 int ds_raster_destroy(ds_raster *r);
 
+/* Forward rasterization that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot let a library call cudaMalloc: an
+ * application whose own pool allocator owns all device memory, or a per-frame
+ * loop in which cudaMalloc / cudaFree would synchronise the device.  Same
+ * kernels and same image as ds_raster_create + ds_raster_forward, with every
+ * intermediate buffer in one ~5.7 MB __device__ array of the library that each
+ * GPU holds until the process exits.  Limits: count <= 8192 splats,
+ * width * height <= 65536 pixels, at most 1024 16x16 tiles (DS_ERR_ARG
+ * beyond); (tile, splat) pairs beyond 131072 are dropped.  All calls on a
+ * device share the array, so calls that overlap on the GPU race: issue them on
+ * one stream.  The first call on each device looks up the array's device
+ * address; make it before any stream capture.  Asynchronous. */
+int ds_raster_forward_noalloc(const ds_splat2d *in, int width, int height, float *out_rgb,
+                              ds_stream stream);
+
 /* ---- Loss: replaces MSELossLayer::forward / ::backward / ::getLoss
  *      (src/layers/mse_loss_layer.cu:85-92, :94-99, :101-105).
  *      L = sum_px sum_c (r - t)^2 / num_pixels  (normalised by pixels, not pixels*3).
