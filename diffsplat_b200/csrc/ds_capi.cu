@@ -45,7 +45,26 @@ bool s2_ok(const ds_splat2d* s) {
 
 }  // namespace
 
+namespace {
+int g_default_grad_mode = -1;  // -1: not yet read from the environment
+}
+
 extern "C" {
+
+int ds_default_grad_mode(void) {
+  if (g_default_grad_mode < 0) {
+    const char* e = getenv("DS_GRAD_MODE");
+    g_default_grad_mode =
+        (e && strcmp(e, "exact") == 0) ? DS_GRAD_EXACT : DS_GRAD_REFERENCE;
+  }
+  return g_default_grad_mode;
+}
+
+int ds_set_default_grad_mode(int mode) {
+  if (mode != DS_GRAD_REFERENCE && mode != DS_GRAD_EXACT) return DS_ERR_ARG;
+  g_default_grad_mode = mode;
+  return DS_OK;
+}
 
 int ds_abi_version(void) { return DS_ABI_VERSION; }
 
@@ -97,7 +116,7 @@ int ds_project_forward(const ds_splat3d* in, const float pv[16], const ds_splat2
 int ds_project_backward(const ds_splat3d* in, const float pv[16], const ds_splat2d* grad_out,
                         const ds_splat3d* grad_in, ds_stream stream) {
   if (!pv || !s3_ok(in) || !s2_ok(grad_out) || !s3_ok(grad_in)) return DS_ERR_ARG;
-  return ds::launch_project_backward(*in, pv, *grad_out, *grad_in, DS_GRAD_REFERENCE,
+  return ds::launch_project_backward(*in, pv, *grad_out, *grad_in, ds_default_grad_mode(),
                                      (cudaStream_t)stream);
 }
 
@@ -115,6 +134,7 @@ int ds_raster_create(int width, int height, int max_splats, int64_t max_isects, 
   ds_raster* r = new (std::nothrow) ds_raster();
   if (!r) return DS_ERR_OOM;
   int st = ds::raster_alloc(r->rb, width, height, max_splats, max_isects);
+  r->rb.grad_mode = ds_default_grad_mode();
   if (st != DS_OK) {
     ds::raster_free(r->rb);
     delete r;

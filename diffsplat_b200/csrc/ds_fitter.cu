@@ -427,7 +427,7 @@ int ds_fitter_default_config(ds_fitter_config* cfg) {
   cfg->epsilon = 1e-8f;
   cfg->storage = DS_STORAGE_FP32;
   cfg->use_graph = 1;
-  cfg->grad_mode = DS_GRAD_REFERENCE;
+  cfg->grad_mode = ds_default_grad_mode();
   return DS_OK;
 }
 

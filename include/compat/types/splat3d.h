@@ -1,0 +1,28 @@
+// World-space splats after activation and their gradients (src/types/splat3d.h:14-51).
+#pragma once
+#include "gpu_soa.h"
+
+struct Splat3DParams : GpuSoA {
+  CudaBuffer<float> pos_x, pos_y, pos_z;
+  CudaBuffer<float> cov_xx, cov_xy, cov_xz;
+  CudaBuffer<float> cov_yy, cov_yz, cov_zz;
+  CudaBuffer<float> color_r, color_g, color_b;
+  CudaBuffer<float> opacity;
+  std::vector<CudaBuffer<float>*> fields() override {
+    return {&pos_x,  &pos_y,  &pos_z,   &cov_xx,  &cov_xy,  &cov_xz, &cov_yy,
+            &cov_yz, &cov_zz, &color_r, &color_g, &color_b, &opacity};
+  }
+};
+
+struct Splat3DGrads : GpuSoA {
+  CudaBuffer<float> grad_pos_x, grad_pos_y, grad_pos_z;
+  CudaBuffer<float> grad_cov_xx, grad_cov_xy, grad_cov_xz;
+  CudaBuffer<float> grad_cov_yy, grad_cov_yz, grad_cov_zz;
+  CudaBuffer<float> grad_color_r, grad_color_g, grad_color_b;
+  CudaBuffer<float> grad_opacity;
+  std::vector<CudaBuffer<float>*> fields() override {
+    return {&grad_pos_x,  &grad_pos_y,  &grad_pos_z,   &grad_cov_xx,  &grad_cov_xy,
+            &grad_cov_xz, &grad_cov_yy, &grad_cov_yz,  &grad_cov_zz,  &grad_color_r,
+            &grad_color_g, &grad_color_b, &grad_opacity};
+  }
+};

@@ -80,6 +80,13 @@ typedef struct ds_splat2d {
   int32_t count;
 } ds_splat2d;
 
+/* Process-wide default gradient mode, used by new raster handles, by
+ * ds_fitter_default_config, by ds_project_backward and by the drop-in C++
+ * layers.  Initialised from the environment variable DS_GRAD_MODE
+ * ("reference" or "exact"; DS_GRAD_REFERENCE when unset). */
+int ds_set_default_grad_mode(int mode);
+int ds_default_grad_mode(void);
+
 /* Library information. */
 int ds_abi_version(void);
 const char *ds_status_string(int status);
