@@ -113,15 +113,32 @@ def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
-    return {"hbm_gbs": 6650.0, "src": "fallback"}
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "sm_max_mhz": d.get("sm_max_mhz", 1965.0),
+                "src": "measured"}
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0, "src": "fallback"}
+
+
+def fp32_peak_tflops(sm_mhz: float) -> float:
+    """Non-tensor FP32 peak: SMs x 128 lanes x 2 (FMA) x SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    return sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+# FP32 operations per contributing (pixel, splat) pair, counted from the kernels'
+# per-pixel code (an FMA is 2): forward 24 (+1 exp), backward 70 (+1 exp, 1 rcp).
+FLOPS_PER_PAIR = {"composite_fwd": 24, "composite_bwd": 70}
+
+# DRAM bytes (read + write) per (tile, splat) pair of one composite launch, from
+# an ncu capture of the same 1280x720 / 60000-splat workload, scaled by pairs.
+NCU_DRAM_BYTES_PER_ISECT = {}
 
 
 def kernels_per_step(tiles: int) -> int:
     passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
     # step_begin, preprocess, 4 depth passes x 3, scan x 3, emit, tile passes x 3,
-    # ranges, composite fwd, composite bwd, backward+Adam
-    return 2 + 12 + 3 + 1 + 3 * passes + 1 + 3
+    # ranges, tile schedule, composite fwd, composite bwd, segment reduce, backward+Adam
+    return 2 + 12 + 3 + 1 + 3 * passes + 2 + 4
 
 
 def stage_bytes(n: int, isects: int, pixels: int, tiles: int) -> dict:
@@ -138,20 +155,24 @@ def stage_bytes(n: int, isects: int, pixels: int, tiles: int) -> dict:
     }
 
 
-def cpu_baseline_oracle(prob) -> dict:
-    """FP64 oracle: one fwd+bwd (+ Adam) step of the same workload on all host cores."""
+def cpu_baseline_oracle(prob, budget_s: float = 10.0) -> dict:
+    """FP64 oracle: fwd+bwd+Adam steps of the same workload from its initial state
+    on all host cores, as many as fit in about budget_s seconds."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     P = prob.params.astype(np.float64)
+    m, v = np.zeros_like(P), np.zeros_like(P)
     t0 = time.perf_counter()
-    fw, gp = O.loss_and_grads(P, prob.sh_degree, prob.cam, prob.pv, prob.width, prob.height,
-                              prob.target, threads=threads)
-    m = np.zeros_like(P)
-    O.adam(P, gp, m, m.copy(), 1e-3, 1)
+    steps = 0
+    while steps == 0 or time.perf_counter() - t0 < budget_s:
+        fw, gp = O.loss_and_grads(P, prob.sh_degree, prob.cam, prob.pv, prob.width, prob.height,
+                                  prob.target, threads=threads)
+        P, m, v = O.adam(P, gp, m, v, 1e-3, steps + 1)
+        steps += 1
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": "1 fwd+bwd+Adam step of the same 1280x720 / 60000-splat workload "
-                      f"({dt:.2f} s)"}
+    return {"value": steps / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} fwd+bwd+Adam steps of the same 1280x720 / 60000-splat workload "
+                      f"from its initial state ({dt:.1f} s)"}
 
 
 def run_ours(args, world, rank, local):
@@ -161,13 +182,22 @@ def run_ours(args, world, rank, local):
 
     prob = reference_default(seed=rank)
     n = prob.params.shape[1]
-    f = api.Fitter(prob.width, prob.height, n, prob.sh_degree, lrs=prob.lrs)
-    f.set_params(prob.params)
-    f.set_target(torch.tensor(prob.target, device="cuda"))
-    f.set_camera(prob.pv, prob.cam)
+    tgt = torch.tensor(prob.target, device="cuda")
+
+    def make():
+        f = api.Fitter(prob.width, prob.height, n, prob.sh_degree, lrs=prob.lrs)
+        f.set_params(prob.params)
+        f.set_target(tgt)
+        f.set_camera(prob.pv, prob.cam)
+        return f
+
+    # Device-timed arm and end-to-end arm run the same trajectory (same initial
+    # state, same warm-up), so both time the same per-step work.
+    f, g = make(), make()
     flush = torch.empty(FLUSH_BYTES // 4, device="cuda")
     for _ in range(args.warmup):
         f.step(1)
+        g.step(1)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
@@ -184,18 +214,22 @@ def run_ours(args, world, rank, local):
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     t_max = max_over_ranks(world, t_ms)
     loss = f.loss()
-    # end to end through the public API: camera upload, step, loss readback each step
+    # end to end through the public API: camera upload (H2D), step, loss readback
+    # (D2H) each step
+    cam_pv = torch.tensor(prob.pv).pin_memory()
+    cam_pos = torch.tensor(prob.cam).pin_memory()
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
     for k in range(args.steps):
         flush.fill_(float(k))
         e2e_ev[k][0].record()
-        f.set_camera(prob.pv, prob.cam)
-        f.step(1)
-        f.loss()
+        g.set_camera(cam_pv.numpy(), cam_pos.numpy())
+        g.step(1)
+        g.loss()
         e2e_ev[k][1].record()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(world, sum(a.elapsed_time(b) for a, b in e2e_ev))
+    g.close()
     # per-stage device times (eager step with events between stages)
     stages = {s: 0.0 for s in api.Fitter.STAGES}
     reps = 5
@@ -204,10 +238,12 @@ def run_ours(args, world, rank, local):
         for s, v in f.profile_step().items():
             stages[s] += v / reps
     cnt = f.counters()
+    pairs = f.pair_stats()
     code, flags = f.status()
     f.close()
     out = dict(t_ms=t_max, e2e_ms=e2e_ms, loss=loss, psnr=psnr_from_ref_loss(loss),
-               stages=stages, counters=cnt, clocks=clk.summary(), status=code, prob=prob)
+               stages=stages, counters=cnt, pairs=pairs, clocks=clk.summary(), status=code,
+               prob=prob)
     return out
 
 
@@ -256,7 +292,9 @@ def profile_run(args):
     f.step(args.warmup + args.steps)
     torch.cuda.synchronize()
     code, flags = f.status()
-    print(f"profile run: {args.warmup + args.steps} steps, loss {f.loss():.6f}, status {code}")
+    cnt = f.counters()
+    print(f"profile run: {args.warmup + args.steps} steps, loss {f.loss():.6f}, status {code}, "
+          f"pairs of the last step {cnt['n_isects']}")
     f.close()
     if code != 0:
         sys.exit(1)
@@ -265,8 +303,8 @@ def profile_run(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
@@ -320,7 +358,11 @@ def main():
     stages = r["stages"]
     dom = max(stages, key=stages.get)
     peaks = measured_peaks()
-    achieved = sb[dom] / (stages[dom] * 1e-3) / 1e9
+    pairs = r["pairs"]["contributing"]
+    fp32_peak = fp32_peak_tflops(r["clocks"].get("sm_max_mhz") or peaks["sm_max_mhz"])
+    tflops = {k: pairs * FLOPS_PER_PAIR[k] / (stages[k] * 1e-3) / 1e12 for k in FLOPS_PER_PAIR}
+    gbs = sb[dom] / (stages[dom] * 1e-3) / 1e9
+    traffic = NCU_DRAM_BYTES_PER_ISECT.get(dom)
     line.update({
         "value": value, "ms_per_step": r["t_ms"] / args.steps,
         "mpix_per_s": value * pixels / 1e6,
@@ -328,10 +370,18 @@ def main():
                 "h2d_bytes_per_step": 80, "d2h_bytes_per_step": 4},
         "gpu_launches": kernels_per_step(tiles) * args.steps,
         "clocks": r["clocks"],
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
-                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                     "traffic": None, "peak_src": peaks["src"],
-                     "algorithmic_bytes": sb[dom]},
+        "roofline": {"bound": "fp32", "kernel": dom, "achieved": tflops.get(dom),
+                     "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": tflops[dom] / fp32_peak if dom in tflops else None,
+                     "traffic": traffic * isects if traffic else None,
+                     "peak_src": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock",
+                     "algorithmic_flops": pairs * FLOPS_PER_PAIR.get(dom, 0),
+                     "contributing_pairs": pairs,
+                     "evaluated_pairs": r["pairs"]["evaluated"],
+                     "composite_fwd_tflops": tflops["composite_fwd"],
+                     "hbm": {"achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                             "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
+                             "algorithmic_bytes": sb[dom]}},
         "stage_ms": stages, "n_isects": isects, "visible": r["counters"]["visible"],
         "final_loss": r["loss"], "status": r["status"],
     })

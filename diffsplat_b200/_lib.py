@@ -24,6 +24,8 @@ DS_GRAD_EXACT = 1
 
 DS_STORAGE_FP32 = 0
 DS_STORAGE_BF16 = 1
+DS_SCHEDULE_LONGEST_FIRST = 0
+DS_SCHEDULE_RASTER = 1
 
 DS_RASTER_KEYS = 0
 DS_RASTER_IDS = 1
@@ -67,7 +69,8 @@ class FitterConfig(C.Structure):
                 ("lr_pos", C.c_float), ("lr_scale", C.c_float), ("lr_rot", C.c_float),
                 ("lr_sh_dc", C.c_float), ("lr_sh_rest", C.c_float), ("lr_opacity", C.c_float),
                 ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float),
-                ("storage", C.c_int32), ("use_graph", C.c_int32), ("grad_mode", C.c_int32)]
+                ("storage", C.c_int32), ("use_graph", C.c_int32), ("grad_mode", C.c_int32),
+                ("schedule", C.c_int32)]
 
 
 GAUSSIAN3D_FIELDS = ("pos_x", "pos_y", "pos_z", "scale_x", "scale_y", "scale_z",
@@ -119,6 +122,8 @@ _SIGS = {
     "ds_fitter_destroy": (C.c_int, [_vp]),
     "ds_fitter_profile_step": (C.c_int, [_vp, _fp, C.c_int, _vp]),
     "ds_fitter_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
+    "ds_fitter_pair_stats": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int, _vp]),
+    "ds_fitter_params_updated": (C.c_int, [_vp]),
 }
 
 _lib = None

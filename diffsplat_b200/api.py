@@ -239,7 +239,7 @@ class Fitter:
     def __init__(self, width: int, height: int, count: int, sh_degree: int = 0, lrs=None,
                  max_isects: int = 0, use_graph: bool = True, keep_grads: bool = False,
                  storage: int = L.DS_STORAGE_FP32, betas=(0.9, 0.999), eps: float = 1e-8,
-                 grad_mode: int = L.DS_GRAD_REFERENCE):
+                 grad_mode: int = L.DS_GRAD_REFERENCE, schedule: int | None = None):
         cfg = L.FitterConfig()
         L.call("ds_fitter_default_config", C.byref(cfg))
         cfg.width, cfg.height, cfg.count, cfg.sh_degree = width, height, count, sh_degree
@@ -252,6 +252,8 @@ class Fitter:
         cfg.storage = storage
         cfg.use_graph = 1 if use_graph else 0
         cfg.grad_mode = grad_mode
+        if schedule is not None:
+            cfg.schedule = schedule
         h = C.c_void_p()
         L.call("ds_fitter_create_with_grads" if keep_grads else "ds_fitter_create", C.byref(cfg),
                C.byref(h))
@@ -276,6 +278,7 @@ class Fitter:
 
     def set_params(self, params) -> None:
         self.params.copy_(torch.as_tensor(params, device="cuda"))
+        L.call("ds_fitter_params_updated", self.h)
 
     def set_target(self, target: torch.Tensor, stream=None) -> None:
         target = target.contiguous()
@@ -326,3 +329,10 @@ class Fitter:
         out = (C.c_uint64 * 3)()
         L.call("ds_fitter_counters", self.h, out, 3)
         return {"n_isects": int(out[0]), "visible": int(out[1]), "step": int(out[2])}
+
+    def pair_stats(self) -> dict:
+        """(pixel, splat) pairs of the most recent step's composite: those that
+        contribute and those the kernel evaluates."""
+        out = (C.c_uint64 * 2)()
+        L.call("ds_fitter_pair_stats", self.h, out, 2, _stream())
+        return {"contributing": int(out[0]), "evaluated": int(out[1])}

@@ -6,6 +6,7 @@
 // to the reference CUDA build, and this file is compiled with the same
 // --use_fast_math flag the reference uses (CMakeLists.txt:121-127).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -131,28 +132,35 @@ struct ShBasis {
   float y[15];
 };
 
-__device__ __forceinline__ float sh_channel(float dc, const float* __restrict__ rest, int stride,
+// Loads of a stored attribute as FP32 (FP32 or BF16 storage).
+__device__ __forceinline__ float ldv(float x) { return x; }
+__device__ __forceinline__ float ldv(__nv_bfloat16 x) { return __bfloat162float(x); }
+
+template <typename T>
+__device__ __forceinline__ float sh_channel(float dc, const T* __restrict__ rest, int stride,
                                             int degree, float3 v) {
   float c = dc * kC0;
   if (degree >= 1) {
-    c += kC1 * (-v.y * rest[0 * stride] + v.z * rest[1 * stride] - v.x * rest[2 * stride]);
+    c += kC1 * (-v.y * ldv(rest[0 * stride]) + v.z * ldv(rest[1 * stride]) -
+                v.x * ldv(rest[2 * stride]));
   }
   if (degree >= 2) {
     float xx = v.x * v.x, yy = v.y * v.y, zz = v.z * v.z;
     float xy = v.x * v.y, yz = v.y * v.z, xz = v.x * v.z;
-    c += kC2_0 * xy * rest[3 * stride] + kC2_1 * yz * rest[4 * stride] +
-         kC2_2 * (2 * zz - xx - yy) * rest[5 * stride] + kC2_3 * xz * rest[6 * stride] +
-         kC2_4 * (xx - yy) * rest[7 * stride];
+    c += kC2_0 * xy * ldv(rest[3 * stride]) + kC2_1 * yz * ldv(rest[4 * stride]) +
+         kC2_2 * (2 * zz - xx - yy) * ldv(rest[5 * stride]) + kC2_3 * xz * ldv(rest[6 * stride]) +
+         kC2_4 * (xx - yy) * ldv(rest[7 * stride]);
   }
   if (degree >= 3) {
     float xx = v.x * v.x, yy = v.y * v.y, zz = v.z * v.z;
     float xy = v.x * v.y;
-    c += kC3_0 * v.y * (3 * xx - yy) * rest[8 * stride] + kC3_1 * xy * v.z * rest[9 * stride] +
-         kC3_2 * v.y * (4 * zz - xx - yy) * rest[10 * stride] +
-         kC3_3 * v.z * (2 * zz - 3 * xx - 3 * yy) * rest[11 * stride] +
-         kC3_4 * v.x * (4 * zz - xx - yy) * rest[12 * stride] +
-         kC3_5 * v.z * (xx - yy) * rest[13 * stride] +
-         kC3_6 * v.x * (xx - 3 * yy) * rest[14 * stride];
+    c += kC3_0 * v.y * (3 * xx - yy) * ldv(rest[8 * stride]) +
+         kC3_1 * xy * v.z * ldv(rest[9 * stride]) +
+         kC3_2 * v.y * (4 * zz - xx - yy) * ldv(rest[10 * stride]) +
+         kC3_3 * v.z * (2 * zz - 3 * xx - 3 * yy) * ldv(rest[11 * stride]) +
+         kC3_4 * v.x * (4 * zz - xx - yy) * ldv(rest[12 * stride]) +
+         kC3_5 * v.z * (xx - yy) * ldv(rest[13 * stride]) +
+         kC3_6 * v.x * (xx - 3 * yy) * ldv(rest[14 * stride]);
   }
   return c;
 }

@@ -15,6 +15,7 @@
 // in shared memory and sums the warps in a fixed order: gradients are
 // deterministic run to run.
 #include <stdlib.h>
+#include <string.h>
 
 #include "ds_common.cuh"
 #include "ds_internal.h"
@@ -80,33 +81,49 @@ __device__ __forceinline__ Pixels<PPT> pixels(int tile, int ntx, int W, int H) {
   return m;
 }
 
-template <int PPT>
-__device__ __forceinline__ bool misses(const float4& a, const Pixels<PPT>& m) {
-  return a.x + a.z < m.wx_lo || a.x - a.z > m.wx_hi || a.y + a.w < m.wy_lo ||
-         a.y - a.w > m.wy_hi;
+// Acceptance-box test of a splat record against one warp's pixel box
+// {x_lo, x_hi, y_lo, y_hi}.
+__device__ __forceinline__ bool misses(const float4& a, const float4& box) {
+  return a.x + a.z < box.x || a.x - a.z > box.y || a.y + a.w < box.z || a.y - a.w > box.w;
 }
 
-template <int PPT, bool kLoss>
+// Bit w set: the splat's acceptance box overlaps warp w's pixel block.
+template <int NW>
+__device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4* box) {
+  uint32_t mk = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) mk |= misses(a, box[w]) ? 0u : (1u << w);
+  return mk;
+}
+
+template <int PPT, bool kLoss, bool kCount = false>
 __global__ void __launch_bounds__(Lay<PPT>::kThreads)
     composite_fwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const uint32_t* __restrict__ sorted_splat,
-                         const int2* __restrict__ ranges, float* __restrict__ out_rgb,
-                         float* __restrict__ out_alpha, int32_t* __restrict__ last_ids, int W,
-                         int H, int ntx, const float* __restrict__ target,
-                         float* __restrict__ loss_partials, DevScalars* __restrict__ sc) {
+                         const int2* __restrict__ ranges, const int32_t* __restrict__ order,
+                         float* __restrict__ out_rgb, float* __restrict__ out_alpha,
+                         int32_t* __restrict__ last_ids, int W, int H, int ntx,
+                         const float* __restrict__ target, float* __restrict__ loss_partials,
+                         DevScalars* __restrict__ sc) {
   using Lc = Lay<PPT>;
   constexpr int NT = Lc::kThreads;
+  constexpr int NW = Lc::kWarps;
   __shared__ float4 sA[kFwdBatch], sB[kFwdBatch], sC[kFwdBatch];
-  __shared__ float red[Lc::kWarps];
+  __shared__ uint32_t sMask[kFwdBatch];
+  __shared__ float4 sBox[NW];
+  __shared__ float red[NW];
   __shared__ bool last;
-  const int tile = blockIdx.x;
+  const int tile = order ? order[blockIdx.x] : (int)blockIdx.x;
   const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
   const int2 range = ranges[tile];
   const int start = range.x, end = range.y;
   float T[PPT], Cr[PPT], Cg[PPT], Cb[PPT];
   uint32_t cur[PPT];
   bool done[PPT];
   bool all_done = true;
+  uint32_t n_contrib = 0, n_tested = 0;
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     T[k] = 1.f;
@@ -117,32 +134,44 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   }
   for (int b0 = start; b0 < end; b0 += kFwdBatch) {
     if (__syncthreads_count(all_done) >= NT) break;
+    // Stage the batch; each splat's warp-overlap mask is computed once here
+    // so that every warp walks only the splats that can touch its pixels.
     for (int l = threadIdx.x; l < kFwdBatch; l += NT) {
       const int idx = b0 + l;
+      uint32_t mk = 0u;
       if (idx < end) {
         const uint32_t g = sorted_splat[idx];
-        sA[l] = ra[g];
+        const float4 a = ra[g];
+        sA[l] = a;
         sB[l] = rb[g];
         sC[l] = rc[g];
+        mk = warp_hits<NW>(a, sBox);
       }
+      sMask[l] = mk;
     }
     __syncthreads();
     const int bs = min(kFwdBatch, end - b0);
-    if (__any_sync(0xffffffffu, !all_done)) {
-      for (int t = 0; t < bs; ++t) {
+    bool stop = !__any_sync(0xffffffffu, !all_done);
+    for (int kw = 0; kw * 32 < bs && !stop; ++kw) {
+      const int l = kw * 32 + lane;
+      uint32_t word = __ballot_sync(0xffffffffu, l < bs && ((sMask[l] >> w) & 1u));
+      while (word) {
+        const int t = kw * 32 + __ffs(word) - 1;
+        word &= word - 1u;
         const float4 a = sA[t];
-        if (misses<PPT>(a, m)) continue;
         const float4 b = sB[t];
         const float4 c = sC[t];
         const float dx = a.x - m.px;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
           if (done[k]) continue;
+          if (kCount) ++n_tested;
           const float dy = a.y - m.py[k];
           const float sigma = 0.5f * conic_dist2(dx, dy, b.x, b.y, b.z);
           if (sigma < 0.f || sigma > c.w) continue;
           const float alpha = fminf(kMaxAlpha, b.w * __expf(-sigma));
           if (alpha < kAlphaThres) continue;
+          if (kCount) ++n_contrib;
           const float vis = alpha * T[k];
           Cr[k] = __fmaf_rn(c.x, vis, Cr[k]);
           Cg[k] = __fmaf_rn(c.y, vis, Cg[k]);
@@ -154,8 +183,23 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
         all_done = true;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) all_done = all_done && done[k];
-        if (!__any_sync(0xffffffffu, !all_done)) break;
+        if (!__any_sync(0xffffffffu, !all_done)) {
+          stop = true;
+          break;
+        }
       }
+    }
+  }
+  if (kCount) {
+    uint32_t a = n_contrib, t = n_tested;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&sc->pairs[0], (unsigned long long)a);
+      atomicAdd(&sc->pairs[1], (unsigned long long)t);
     }
   }
   float l = 0.f;
@@ -213,7 +257,8 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
                          const float4* __restrict__ rc, const float* __restrict__ ridet,
                          const uint32_t* __restrict__ sorted_splat,
                          const uint32_t* __restrict__ sorted_emit, const int2* __restrict__ ranges,
-                         const float* __restrict__ alphas, const int32_t* __restrict__ last_ids,
+                         const int32_t* __restrict__ order, const float* __restrict__ alphas,
+                         const int32_t* __restrict__ last_ids,
                          const float* __restrict__ grad_or_image, const float* __restrict__ target,
                          float* __restrict__ isect_grad, int W, int H, int ntx) {
   using Lc = Lay<PPT>;
@@ -222,13 +267,16 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   constexpr int B = Lc::kBwdBatch;
   __shared__ float4 sA[B], sB[B], sC[B];
   __shared__ float sI[B];
+  __shared__ uint32_t sMask[B];
+  __shared__ float4 sBox[NW];
   __shared__ __align__(16) float part[NW][B * 9];  // per-warp partial of each batch splat
-  const int tile = blockIdx.x;
+  const int tile = order ? order[blockIdx.x] : (int)blockIdx.x;
   const int2 range = ranges[tile];
   const int start = range.x, end = range.y;
   if (end <= start) return;
   const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
   float T[PPT], gr[PPT], gg[PPT], gb[PPT], accr[PPT], accg[PPT], accb[PPT];
   int32_t fin[PPT];
   int32_t my_final = -1;
@@ -262,13 +310,17 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
     // stage the batch back to front: slot l holds sorted index batch_end - l
     for (int l = threadIdx.x; l < B; l += NT) {
       const int li = batch_end - l;
+      uint32_t mk = 0u;
       if (li >= start) {
         const uint32_t g = sorted_splat[li];
-        sA[l] = ra[g];
+        const float4 a = ra[g];
+        sA[l] = a;
         sB[l] = rb[g];
         sC[l] = rc[g];
         sI[l] = ridet[g];
+        mk = warp_hits<NW>(a, sBox);
       }
+      sMask[l] = mk;
     }
     {
       float4* p4 = reinterpret_cast<float4*>(&part[0][0]);
@@ -276,63 +328,69 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
     }
     __syncthreads();
     const int t_start = max(0, batch_end - warp_final);
-    for (int t = t_start; t < bs; ++t) {
-      const float4 a = sA[t];
-      if (misses<PPT>(a, m)) continue;
-      const float4 b = sB[t];
-      const float4 c = sC[t];
-      const float idet = sI[t];
-      const float dx = a.x - m.px;
-      const int sidx = batch_end - t;
-      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      float va = 0.f;
-      bool any = false;
+    for (int kw = 0; kw * 32 < bs; ++kw) {
+      const int l = kw * 32 + lane;
+      uint32_t word =
+          __ballot_sync(0xffffffffu, l >= t_start && l < bs && ((sMask[l] >> w) & 1u));
+      while (word) {
+        const int t = kw * 32 + __ffs(word) - 1;
+        word &= word - 1u;
+        const float4 a = sA[t];
+        const float4 b = sB[t];
+        const float4 c = sC[t];
+        const float idet = sI[t];
+        const float dx = a.x - m.px;
+        const int sidx = batch_end - t;
+        float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float va = 0.f;
+        bool any = false;
 #pragma unroll
-      for (int k = 0; k < PPT; ++k) {
-        if (!(m.inside[k] && sidx <= fin[k])) continue;
-        const float dy = a.y - m.py[k];
-        const float dist2 = conic_dist2(dx, dy, b.x, b.y, b.z);
-        const float sigma = 0.5f * dist2;
-        if (sigma < 0.f || sigma > c.w) continue;
-        const float opac = b.w;
-        const float g_exp = __expf(-sigma);
-        const float alpha = fminf(kMaxAlpha, opac * g_exp);
-        if (alpha < kAlphaThres) continue;
-        any = true;
-        const float T_before = T[k] / fmaxf(1.f - alpha, 1e-6f);
-        const float fac = alpha * T_before;
-        v[0] += fac * gr[k];
-        v[1] += fac * gg[k];
-        v[2] += fac * gb[k];
-        // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
-        // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
-        // exact derivative divides it by T_after instead.
-        const float ia = kExact ? 1.f / T[k] : 1.f;
-        const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
-                                          (c.y - accg[k] * ia) * gg[k] +
-                                          (c.z - accb[k] * ia) * gb[k]);
-        if (opac * g_exp <= kMaxAlpha) {
-          va += g_exp * v_alpha;
-          const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
-          const float ddx = 2.f * (dx * b.x + dy * b.y);
-          const float ddy = 2.f * (dx * b.y + dy * b.z);
-          v[3] += v_dist2 * ddx;
-          v[4] += v_dist2 * ddy;
-          v[5] += v_dist2 * (-0.25f * ddx * ddx);
-          v[7] += v_dist2 * (-0.25f * ddy * ddy);
-          v[6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * idet);
+        for (int k = 0; k < PPT; ++k) {
+          if (!(m.inside[k] && sidx <= fin[k])) continue;
+          const float dy = a.y - m.py[k];
+          const float dist2 = conic_dist2(dx, dy, b.x, b.y, b.z);
+          const float sigma = 0.5f * dist2;
+          if (sigma < 0.f || sigma > c.w) continue;
+          const float opac = b.w;
+          const float g_exp = __expf(-sigma);
+          const float alpha = fminf(kMaxAlpha, opac * g_exp);
+          if (alpha < kAlphaThres) continue;
+          any = true;
+          const float T_before = T[k] / fmaxf(1.f - alpha, 1e-6f);
+          const float fac = alpha * T_before;
+          v[0] += fac * gr[k];
+          v[1] += fac * gg[k];
+          v[2] += fac * gb[k];
+          // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
+          // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
+          // exact derivative divides it by T_after instead.
+          const float ia = kExact ? 1.f / T[k] : 1.f;
+          const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
+                                            (c.y - accg[k] * ia) * gg[k] +
+                                            (c.z - accb[k] * ia) * gb[k]);
+          if (opac * g_exp <= kMaxAlpha) {
+            va += g_exp * v_alpha;
+            const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
+            const float ddx = 2.f * (dx * b.x + dy * b.y);
+            const float ddy = 2.f * (dx * b.y + dy * b.z);
+            v[3] += v_dist2 * ddx;
+            v[4] += v_dist2 * ddy;
+            v[5] += v_dist2 * (-0.25f * ddx * ddx);
+            v[7] += v_dist2 * (-0.25f * ddy * ddy);
+            v[6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * idet);
+          }
+          accr[k] += c.x * fac;
+          accg[k] += c.y * fac;
+          accb[k] += c.z * fac;
+          T[k] = T_before;
         }
-        accr[k] += c.x * fac;
-        accg[k] += c.y * fac;
-        accb[k] += c.z * fac;
-        T[k] = T_before;
+        if (!__any_sync(0xffffffffu, any)) continue;
+        // lane 4q ends up with the warp sum of v[q]
+        const float s8 = warp_sum8_transposed(v, lane);
+        const float sa = warp_sum(va);
+        if ((lane & 3) == 0) part[w][t * 9 + (lane >> 2)] = s8;
+        if (lane == 0) part[w][t * 9 + 8] = sa;
       }
-      if (!__any_sync(0xffffffffu, any)) continue;
-      // lane 4q ends up with the warp sum of v[q]
-      const float s8 = warp_sum8_transposed(v, lane);
-      const float sa = warp_sum(va);
-      if ((lane & 3) == 0) part[w][t * 9 + (lane >> 2)] = s8;
-      if (lane == 0) part[w][t * 9 + 8] = sa;
     }
     __syncthreads();
     for (int l = threadIdx.x; l < bs; l += NT) {
@@ -349,17 +407,29 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   }
 }
 
+const int32_t* schedule(const RasterBuffers& rb) {
+  return rb.schedule == DS_SCHEDULE_LONGEST_FIRST ? rb.tile_order : nullptr;
+}
+
 template <int PPT>
 void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, cudaStream_t s) {
   constexpr int NT = Lay<PPT>::kThreads;
+  const int32_t* order = schedule(rb);
   if (target)
     composite_fwd_kernel<PPT, true><<<rb.tiles, NT, 0, s>>>(
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, out_rgb, rb.alphas,
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,
         rb.last_ids, rb.width, rb.height, rb.ntx, target, rb.loss_partials, rb.scalars);
   else
     composite_fwd_kernel<PPT, false><<<rb.tiles, NT, 0, s>>>(
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, out_rgb, rb.alphas,
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,
         rb.last_ids, rb.width, rb.height, rb.ntx, nullptr, nullptr, rb.scalars);
+}
+
+template <int PPT>
+void launch_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
+  composite_fwd_kernel<PPT, false, true><<<rb.tiles, Lay<PPT>::kThreads, 0, s>>>(
+      rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, schedule(rb), out_rgb,
+      rb.alphas, rb.last_ids, rb.width, rb.height, rb.ntx, nullptr, nullptr, rb.scalars);
 }
 
 template <int PPT>
@@ -369,10 +439,11 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
   const float* g = grad_rgb ? grad_rgb : image;
   const float* t = grad_rgb ? nullptr : target;
   const bool exact = rb.grad_mode == DS_GRAD_EXACT;
+  const int32_t* order = schedule(rb);
 #define DS_BWD(F, E)                                                                         \
   composite_bwd_kernel<PPT, F, E><<<rb.tiles, NT, 0, s>>>(                                   \
       rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit, rb.ranges, \
-      rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx)
+      order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx)
   if (grad_rgb) {
     if (exact) DS_BWD(false, true);
     else DS_BWD(false, false);
@@ -391,7 +462,17 @@ int composite_default_ppt() {
     int v = atoi(e);
     if (v == 1 || v == 2 || v == 4) return v;
   }
-  return 2;  // fastest on the 1280x720 / 60000-splat fitter (sweep of 1, 2, 4 on B200)
+  // Fastest on the 1280x720 / 60000-splat fitter with the longest-first tile
+  // schedule (B200, 1000 steps: 1 -> 688, 2 -> 631, 4 -> 454 steps/s).
+  return 1;
+}
+
+bool composite_longest_first() {
+  static const bool on = [] {
+    const char* e = getenv("DS_TILE_SCHEDULE");
+    return !(e && strcmp(e, "raster") == 0);
+  }();
+  return on;
 }
 
 int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* target,
@@ -400,6 +481,16 @@ int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* tar
     case 4: launch_fwd<4>(rb, out_rgb, target, s); break;
     case 2: launch_fwd<2>(rb, out_rgb, target, s); break;
     default: launch_fwd<1>(rb, out_rgb, target, s); break;
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+int raster_composite_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
+  DS_CUDA(cudaMemsetAsync(rb.scalars->pairs, 0, sizeof(rb.scalars->pairs), s));
+  switch (rb.ppt) {
+    case 4: launch_count<4>(rb, out_rgb, s); break;
+    case 2: launch_count<2>(rb, out_rgb, s); break;
+    default: launch_count<1>(rb, out_rgb, s); break;
   }
   return cuda_status(cudaGetLastError());
 }

@@ -21,6 +21,7 @@
 #include <float.h>
 #include <math.h>
 
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -56,9 +57,38 @@ __global__ void step_begin_kernel(DevScalars* sc, const float2* __restrict__ bc_
   *bc_out = bc;
 }
 
+// Parameter SoA in a storage type T: FP32 (the masters themselves) or BF16
+// (the render copy and Adam moments of the BF16 storage mode).  Field order
+// and layout are those of ds_gaussian3d.
+template <typename T>
+struct Soa {
+  T *pos_x, *pos_y, *pos_z;
+  T *scale_x, *scale_y, *scale_z;
+  T *rot_w, *rot_x, *rot_y, *rot_z;
+  T *sh_dc_r, *sh_dc_g, *sh_dc_b;
+  T *sh_rest_r, *sh_rest_g, *sh_rest_b;
+  T *logit_opacity;
+  int count, sh_num_bands;
+};
+
+Soa<float> soa_of(const ds_gaussian3d& g) {
+  Soa<float> s;
+  s.pos_x = g.pos_x, s.pos_y = g.pos_y, s.pos_z = g.pos_z;
+  s.scale_x = g.scale_x, s.scale_y = g.scale_y, s.scale_z = g.scale_z;
+  s.rot_w = g.rot_w, s.rot_x = g.rot_x, s.rot_y = g.rot_y, s.rot_z = g.rot_z;
+  s.sh_dc_r = g.sh_dc_r, s.sh_dc_g = g.sh_dc_g, s.sh_dc_b = g.sh_dc_b;
+  s.sh_rest_r = g.sh_rest_r, s.sh_rest_g = g.sh_rest_g, s.sh_rest_b = g.sh_rest_b;
+  s.logit_opacity = g.logit_opacity;
+  s.count = g.count, s.sh_num_bands = g.sh_num_bands;
+  return s;
+}
+
+// Preprocess of one step: positions from the FP32 masters P, every other
+// attribute from R (P itself in FP32 storage, the BF16 render copy otherwise).
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
-    fit_preprocess_kernel(ds_gaussian3d P, int degree, const Camera* __restrict__ camp, int W,
-                          int H, int ntx, int nty, float4* __restrict__ ra,
+    fit_preprocess_kernel(ds_gaussian3d P, Soa<T> R, int degree, const Camera* __restrict__ camp,
+                          int W, int H, int ntx, int nty, float4* __restrict__ ra,
                           float4* __restrict__ rb, float4* __restrict__ rc,
                           float* __restrict__ ridet, ushort4* __restrict__ rect,
                           uint32_t* __restrict__ counts, uint32_t* __restrict__ depth_keys,
@@ -79,9 +109,10 @@ __global__ void __launch_bounds__(kThreads)
     float ndc_x = 0.f, ndc_y = 0.f;
     Cov2 c2 = {0.f, 0.f, 0.f};
     if (clip_w > 0.f) {
-      UnitQuat q = unit_quat(P.rot_w[i], P.rot_x[i], P.rot_y[i], P.rot_z[i]);
-      Rot3 R = rot_from_quat(q.w, q.x, q.y, q.z);
-      Cov3 c3 = cov3_from(R, expf(P.scale_x[i]), expf(P.scale_y[i]), expf(P.scale_z[i]));
+      UnitQuat q = unit_quat(ldv(R.rot_w[i]), ldv(R.rot_x[i]), ldv(R.rot_y[i]), ldv(R.rot_z[i]));
+      Rot3 Rm = rot_from_quat(q.w, q.x, q.y, q.z);
+      Cov3 c3 = cov3_from(Rm, expf(ldv(R.scale_x[i])), expf(ldv(R.scale_y[i])),
+                          expf(ldv(R.scale_z[i])));
       const float inv_w = 1.f / clip_w;
       const float inv_w2 = inv_w * inv_w;
       ndc_x = clip_x * inv_w;
@@ -92,16 +123,14 @@ __global__ void __launch_bounds__(kThreads)
       vis = tile_rect(ndc_x, ndc_y, ndc_z, c2.xx, c2.xy, c2.yy, W, H, ntx, nty, r);
       if (vis) {
         float3 v = dir_to_camera(sCam[0], sCam[1], sCam[2], px, py, pz);
-        const float cr =
-            clamp01(sh_channel(P.sh_dc_r[i], degree > 0 ? P.sh_rest_r + i : nullptr, n, degree, v) +
-                    0.5f);
-        const float cg =
-            clamp01(sh_channel(P.sh_dc_g[i], degree > 0 ? P.sh_rest_g + i : nullptr, n, degree, v) +
-                    0.5f);
-        const float cb =
-            clamp01(sh_channel(P.sh_dc_b[i], degree > 0 ? P.sh_rest_b + i : nullptr, n, degree, v) +
-                    0.5f);
-        const float op = 1.f / (1.f + expf(-P.logit_opacity[i]));
+        const T* no = nullptr;
+        const float cr = clamp01(
+            sh_channel(ldv(R.sh_dc_r[i]), degree > 0 ? R.sh_rest_r + i : no, n, degree, v) + 0.5f);
+        const float cg = clamp01(
+            sh_channel(ldv(R.sh_dc_g[i]), degree > 0 ? R.sh_rest_g + i : no, n, degree, v) + 0.5f);
+        const float cb = clamp01(
+            sh_channel(ldv(R.sh_dc_b[i]), degree > 0 ? R.sh_rest_b + i : no, n, degree, v) + 0.5f);
+        const float op = 1.f / (1.f + expf(-ldv(R.logit_opacity[i])));
         Record rec = make_record(ndc_x, ndc_y, c2.xx, c2.xy, c2.yy, cr, cg, cb, op);
         ra[i] = rec.a;
         rb[i] = rec.b;
@@ -130,14 +159,45 @@ __device__ __forceinline__ void adam1(float& p, float& m, float& v, float g, flo
   p -= lr * m_hat / (sqrtf(v_hat) + eps);
 }
 
-__device__ __forceinline__ void adam_at(float* __restrict__ p, float* __restrict__ m,
-                                        float* __restrict__ v, int64_t i, float g, float lr,
-                                        float b1, float b2, float eps, float bc1, float bc2) {
-  float pp = p[i], mm = m[i], vv = v[i];
+// Integer hash "lowbias32" (C. Wellons, 2018): the random bits of the
+// stochastic rounding of BF16 Adam moments, from (element, field, step).
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// FP32 -> BF16 with stochastic rounding: adds 16 random bits below the kept
+// mantissa and truncates, so E[result] = x.  An Adam moment updated by
+// (1 - beta2) = 1e-3 of itself per step would otherwise round back to its old
+// value forever under round-to-nearest (BF16 keeps 8 significant bits).
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t r) {
+  uint32_t u = __float_as_uint(x);
+  if ((u & 0x7f800000u) == 0x7f800000u) return __float2bfloat16_rn(x);
+  u += r & 0xffffu;
+  return __ushort_as_bfloat16((unsigned short)(u >> 16));
+}
+
+__device__ __forceinline__ void store_moment(float* p, float x, uint32_t) { *p = x; }
+__device__ __forceinline__ void store_moment(__nv_bfloat16* p, float x, uint32_t r) {
+  *p = bf16_stochastic(x, r);
+}
+
+// Adam on one element of the FP32 master p with moments of type T; `key`
+// identifies (element, field, step) for the stochastic rounding of BF16 moments.
+template <typename T>
+__device__ __forceinline__ void adam_at(float* __restrict__ p, T* __restrict__ m,
+                                        T* __restrict__ v, int64_t i, float g, float lr, float b1,
+                                        float b2, float eps, float bc1, float bc2, uint32_t key) {
+  float pp = p[i], mm = ldv(m[i]), vv = ldv(v[i]);
   adam1(pp, mm, vv, g, lr, b1, b2, eps, bc1, bc2);
   p[i] = pp;
-  m[i] = mm;
-  v[i] = vv;
+  const uint32_t h = mix32(key ^ mix32((uint32_t)i));
+  store_moment(m + i, mm, h);
+  store_moment(v + i, vv, mix32(h + 0x9e3779b9u));
 }
 
 struct AdamHyper {
@@ -186,11 +246,17 @@ __device__ __forceinline__ void cov_backward(float rw, float rx, float ry, float
   d[6] = nq.inv_norm * (dqz - dot * nq.z);
 }
 
+// Backward of one step and Adam.  P holds the FP32 masters (updated in
+// place), R the attributes the forward rendered (P itself in FP32 storage; in
+// BF16 storage the render copy, rewritten from the updated masters), M and V
+// the moments in the storage type.
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
-    fit_backward_adam_kernel(ds_gaussian3d P, ds_gaussian3d M, ds_gaussian3d V, ds_gaussian3d G,
+    fit_backward_adam_kernel(ds_gaussian3d P, Soa<T> R, Soa<T> M, Soa<T> V, ds_gaussian3d G,
                              int keep_grads, int exact, int degree, const Camera* __restrict__ camp,
-                             const float* __restrict__ g2sum,
-                             const float2* __restrict__ bcp, Lrs lr, AdamHyper h) {
+                             const float* __restrict__ g2sum, const float2* __restrict__ bcp,
+                             const DevScalars* __restrict__ sc, Lrs lr, AdamHyper h) {
+  constexpr bool kBf16 = sizeof(T) == 2;
   __shared__ Mat4 sP;
   __shared__ float sCam[3];
   if (threadIdx.x < 16) sP.m[threadIdx.x] = camp->pv[threadIdx.x];
@@ -200,6 +266,7 @@ __global__ void __launch_bounds__(kThreads)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float2 bc = *bcp;
+  const uint32_t step = kBf16 ? sc->step : 0u;
 
   // 1) Splat2D gradient = sum of this splat's per-tile records (segment_reduce_kernel).
   float g2[9];
@@ -209,6 +276,9 @@ __global__ void __launch_bounds__(kThreads)
 
   // 2) projection backward (persp_project_layer.cu:245-305)
   const float px = P.pos_x[i], py = P.pos_y[i], pz = P.pos_z[i];
+  const float rw = ldv(R.rot_w[i]), rx = ldv(R.rot_x[i]), ry = ldv(R.rot_y[i]),
+              rz = ldv(R.rot_z[i]);
+  const float lsx = ldv(R.scale_x[i]), lsy = ldv(R.scale_y[i]), lsz = ldv(R.scale_z[i]);
   float clip_x, clip_y, clip_z, clip_w;
   project_jacobian(sP, px, py, pz, clip_x, clip_y, clip_z, clip_w);
   float gpos[3] = {0.f, 0.f, 0.f};
@@ -236,9 +306,9 @@ __global__ void __launch_bounds__(kThreads)
     gcol[2] = g2[2];
     gop = g2[8];
     if (exact) {
-      UnitQuat q = unit_quat(P.rot_w[i], P.rot_x[i], P.rot_y[i], P.rot_z[i]);
-      Rot3 R = rot_from_quat(q.w, q.x, q.y, q.z);
-      Cov3 c3 = cov3_from(R, expf(P.scale_x[i]), expf(P.scale_y[i]), expf(P.scale_z[i]));
+      UnitQuat q = unit_quat(rw, rx, ry, rz);
+      Rot3 Rm = rot_from_quat(q.w, q.x, q.y, q.z);
+      Cov3 c3 = cov3_from(Rm, expf(lsx), expf(lsy), expf(lsz));
       float3 e = jacobian_position_grad(sP, J, clip_w, dcxx, hdxy, dcyy, c3.xx, c3.xy, c3.xz,
                                         c3.yy, c3.yz, c3.zz);
       gpos[0] += e.x;
@@ -248,22 +318,24 @@ __global__ void __launch_bounds__(kThreads)
   }
 
   // 3) activation backward (gauss_activ_layer.cu:254-406)
-  const float rw = P.rot_w[i], rx = P.rot_x[i], ry = P.rot_y[i], rz = P.rot_z[i];
-  const float lsx = P.scale_x[i], lsy = P.scale_y[i], lsz = P.scale_z[i];
   float d[7];
   cov_backward(rw, rx, ry, rz, lsx, lsy, lsz, gcov[0], gcov[1], gcov[2], gcov[3], gcov[4],
                gcov[5], d);
   const float3 v = dir_to_camera(sCam[0], sCam[1], sCam[2], px, py, pz);
   float y[15];
   sh_basis(degree, v, y);
-  const float dc_r = P.sh_dc_r[i], dc_g = P.sh_dc_g[i], dc_b = P.sh_dc_b[i];
-  const float col_r = clamp01(sh_channel(dc_r, degree > 0 ? P.sh_rest_r + i : nullptr, n, degree, v) + 0.5f);
-  const float col_g = clamp01(sh_channel(dc_g, degree > 0 ? P.sh_rest_g + i : nullptr, n, degree, v) + 0.5f);
-  const float col_b = clamp01(sh_channel(dc_b, degree > 0 ? P.sh_rest_b + i : nullptr, n, degree, v) + 0.5f);
+  const T* no = nullptr;
+  const float dc_r = ldv(R.sh_dc_r[i]), dc_g = ldv(R.sh_dc_g[i]), dc_b = ldv(R.sh_dc_b[i]);
+  const float col_r =
+      clamp01(sh_channel(dc_r, degree > 0 ? R.sh_rest_r + i : no, n, degree, v) + 0.5f);
+  const float col_g =
+      clamp01(sh_channel(dc_g, degree > 0 ? R.sh_rest_g + i : no, n, degree, v) + 0.5f);
+  const float col_b =
+      clamp01(sh_channel(dc_b, degree > 0 ? R.sh_rest_b + i : no, n, degree, v) + 0.5f);
   const float dR = (col_r > 0.f && col_r < 1.f) ? gcol[0] : 0.f;
   const float dG = (col_g > 0.f && col_g < 1.f) ? gcol[1] : 0.f;
   const float dB = (col_b > 0.f && col_b < 1.f) ? gcol[2] : 0.f;
-  const float logit = P.logit_opacity[i];
+  const float logit = ldv(R.logit_opacity[i]);
   const float s = 1.f / (1.f + expf(-logit));
   const float glogit = gop * s * (1.f - s);
 
@@ -291,39 +363,56 @@ __global__ void __launch_bounds__(kThreads)
   }
 
   // 4) Adam on every field (adam.cu:12-37), group learning rates of
-  //    registerGaussian3DGroups (gaussian3d_adam.h:27-55).
+  //    registerGaussian3DGroups (gaussian3d_adam.h:27-55).  In BF16 storage
+  //    the render copy of every non-position field follows its master.
   const float b1 = h.b1, b2 = h.b2, eps = h.eps, bc1 = bc.x, bc2 = bc.y;
-  adam_at(P.pos_x, M.pos_x, V.pos_x, i, gpos[0], lr.pos, b1, b2, eps, bc1, bc2);
-  adam_at(P.pos_y, M.pos_y, V.pos_y, i, gpos[1], lr.pos, b1, b2, eps, bc1, bc2);
-  adam_at(P.pos_z, M.pos_z, V.pos_z, i, gpos[2], lr.pos, b1, b2, eps, bc1, bc2);
-  adam_at(P.scale_x, M.scale_x, V.scale_x, i, d[0], lr.scale, b1, b2, eps, bc1, bc2);
-  adam_at(P.scale_y, M.scale_y, V.scale_y, i, d[1], lr.scale, b1, b2, eps, bc1, bc2);
-  adam_at(P.scale_z, M.scale_z, V.scale_z, i, d[2], lr.scale, b1, b2, eps, bc1, bc2);
-  adam_at(P.rot_w, M.rot_w, V.rot_w, i, d[3], lr.rot, b1, b2, eps, bc1, bc2);
-  adam_at(P.rot_x, M.rot_x, V.rot_x, i, d[4], lr.rot, b1, b2, eps, bc1, bc2);
-  adam_at(P.rot_y, M.rot_y, V.rot_y, i, d[5], lr.rot, b1, b2, eps, bc1, bc2);
-  adam_at(P.rot_z, M.rot_z, V.rot_z, i, d[6], lr.rot, b1, b2, eps, bc1, bc2);
-  adam_at(P.sh_dc_r, M.sh_dc_r, V.sh_dc_r, i, dR * kC0, lr.sh_dc, b1, b2, eps, bc1, bc2);
-  adam_at(P.sh_dc_g, M.sh_dc_g, V.sh_dc_g, i, dG * kC0, lr.sh_dc, b1, b2, eps, bc1, bc2);
-  adam_at(P.sh_dc_b, M.sh_dc_b, V.sh_dc_b, i, dB * kC0, lr.sh_dc, b1, b2, eps, bc1, bc2);
-  adam_at(P.logit_opacity, M.logit_opacity, V.logit_opacity, i, glogit, lr.opacity, b1, b2, eps,
-          bc1, bc2);
+  uint32_t field = 0;
+  auto upd = [&](float* p, T* m, T* vv, T* r, int64_t k, float g, float l) {
+    adam_at(p, m, vv, k, g, l, b1, b2, eps, bc1, bc2, mix32(step * 32u + field++));
+    if (kBf16 && r) r[k] = __float2bfloat16_rn(p[k]);
+  };
+  upd(P.pos_x, M.pos_x, V.pos_x, nullptr, i, gpos[0], lr.pos);
+  upd(P.pos_y, M.pos_y, V.pos_y, nullptr, i, gpos[1], lr.pos);
+  upd(P.pos_z, M.pos_z, V.pos_z, nullptr, i, gpos[2], lr.pos);
+  upd(P.scale_x, M.scale_x, V.scale_x, R.scale_x, i, d[0], lr.scale);
+  upd(P.scale_y, M.scale_y, V.scale_y, R.scale_y, i, d[1], lr.scale);
+  upd(P.scale_z, M.scale_z, V.scale_z, R.scale_z, i, d[2], lr.scale);
+  upd(P.rot_w, M.rot_w, V.rot_w, R.rot_w, i, d[3], lr.rot);
+  upd(P.rot_x, M.rot_x, V.rot_x, R.rot_x, i, d[4], lr.rot);
+  upd(P.rot_y, M.rot_y, V.rot_y, R.rot_y, i, d[5], lr.rot);
+  upd(P.rot_z, M.rot_z, V.rot_z, R.rot_z, i, d[6], lr.rot);
+  upd(P.sh_dc_r, M.sh_dc_r, V.sh_dc_r, R.sh_dc_r, i, dR * kC0, lr.sh_dc);
+  upd(P.sh_dc_g, M.sh_dc_g, V.sh_dc_g, R.sh_dc_g, i, dG * kC0, lr.sh_dc);
+  upd(P.sh_dc_b, M.sh_dc_b, V.sh_dc_b, R.sh_dc_b, i, dB * kC0, lr.sh_dc);
+  upd(P.logit_opacity, M.logit_opacity, V.logit_opacity, R.logit_opacity, i, glogit,
+      lr.opacity);
   const int nb = P.sh_num_bands;
   const int nb_used = sh_bands(degree);
   for (int b = 0; b < nb; ++b) {
     const int64_t k = (int64_t)b * n + i;
     const float yb = b < nb_used ? y[b] : 0.f;
-    adam_at(P.sh_rest_r, M.sh_rest_r, V.sh_rest_r, k, dR * yb, lr.sh_rest, b1, b2, eps, bc1, bc2);
-    adam_at(P.sh_rest_g, M.sh_rest_g, V.sh_rest_g, k, dG * yb, lr.sh_rest, b1, b2, eps, bc1, bc2);
-    adam_at(P.sh_rest_b, M.sh_rest_b, V.sh_rest_b, k, dB * yb, lr.sh_rest, b1, b2, eps, bc1, bc2);
+    field = 16u + 3u * (uint32_t)b;
+    upd(P.sh_rest_r, M.sh_rest_r, V.sh_rest_r, R.sh_rest_r, k, dR * yb, lr.sh_rest);
+    upd(P.sh_rest_g, M.sh_rest_g, V.sh_rest_g, R.sh_rest_g, k, dG * yb, lr.sh_rest);
+    upd(P.sh_rest_b, M.sh_rest_b, V.sh_rest_b, R.sh_rest_b, k, dB * yb, lr.sh_rest);
   }
 }
 
-// Lays out one ds_gaussian3d view over a single allocation.
-void carve(float* base, int n, int bands, ds_gaussian3d& g) {
-  float** f[14] = {&g.pos_x,   &g.pos_y,   &g.pos_z,   &g.scale_x, &g.scale_y,
-                   &g.scale_z, &g.rot_w,   &g.rot_x,   &g.rot_y,   &g.rot_z,
-                   &g.sh_dc_r, &g.sh_dc_g, &g.sh_dc_b, &g.logit_opacity};
+// Render copy of the BF16 storage mode from the FP32 masters (whole SoA,
+// round to nearest).
+__global__ void __launch_bounds__(kThreads)
+    to_bf16_kernel(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * kThreads)
+    dst[k] = __float2bfloat16_rn(src[k]);
+}
+
+// Lays out one SoA over a single allocation (ds_gaussian3d field order).
+template <typename T>
+void carve_soa(T* base, int n, int bands, Soa<T>& g) {
+  T** f[14] = {&g.pos_x,   &g.pos_y,   &g.pos_z,   &g.scale_x, &g.scale_y,
+               &g.scale_z, &g.rot_w,   &g.rot_x,   &g.rot_y,   &g.rot_z,
+               &g.sh_dc_r, &g.sh_dc_g, &g.sh_dc_b, &g.logit_opacity};
   size_t off = 0;
   for (int k = 0; k < 14; ++k) {
     *f[k] = base + off;
@@ -342,6 +431,20 @@ void carve(float* base, int n, int bands, ds_gaussian3d& g) {
   g.sh_num_bands = bands;
 }
 
+// Lays out one ds_gaussian3d view over a single allocation.
+void carve(float* base, int n, int bands, ds_gaussian3d& g) {
+  Soa<float> t;
+  carve_soa(base, n, bands, t);
+  g.pos_x = t.pos_x, g.pos_y = t.pos_y, g.pos_z = t.pos_z;
+  g.scale_x = t.scale_x, g.scale_y = t.scale_y, g.scale_z = t.scale_z;
+  g.rot_w = t.rot_w, g.rot_x = t.rot_x, g.rot_y = t.rot_y, g.rot_z = t.rot_z;
+  g.sh_dc_r = t.sh_dc_r, g.sh_dc_g = t.sh_dc_g, g.sh_dc_b = t.sh_dc_b;
+  g.sh_rest_r = t.sh_rest_r, g.sh_rest_g = t.sh_rest_g, g.sh_rest_b = t.sh_rest_b;
+  g.logit_opacity = t.logit_opacity;
+  g.count = n;
+  g.sh_num_bands = bands;
+}
+
 }  // namespace
 
 }  // namespace ds
@@ -355,6 +458,10 @@ struct ds_fitter {
   float* v_mem = nullptr;
   float* g_mem = nullptr;
   ds_gaussian3d P{}, M{}, V{}, G{};
+  // BF16 storage: render copy of the masters and the Adam moments
+  __nv_bfloat16* render_mem = nullptr;
+  ds::Soa<__nv_bfloat16> R16{}, M16{}, V16{};
+  bool render_dirty = true;
   float* target = nullptr;
   float* image = nullptr;
   ds::RasterBuffers rb;
@@ -382,9 +489,15 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   step_begin_kernel<<<1, 1, 0, s>>>(rb.scalars, f->bc_table, f->bc_len, f->bc_cur);
   DS_CUDA(cudaGetLastError());
   const int blocks = (n + kThreads - 1) / kThreads;
-  fit_preprocess_kernel<<<blocks, kThreads, 0, s>>>(
-      f->P, f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx, rb.nty, rb.rec_a, rb.rec_b,
-      rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
+  const bool bf16 = f->cfg.storage == DS_STORAGE_BF16;
+  if (bf16)
+    fit_preprocess_kernel<<<blocks, kThreads, 0, s>>>(
+        f->P, f->R16, f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx, rb.nty,
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
+  else
+    fit_preprocess_kernel<<<blocks, kThreads, 0, s>>>(
+        f->P, soa_of(f->P), f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx, rb.nty,
+        rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
   DS_TRY(raster_build_lists(rb, n, s, ev ? ev + 2 : nullptr));
@@ -396,11 +509,28 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   Lrs lr{f->cfg.lr_pos, f->cfg.lr_scale, f->cfg.lr_rot, f->cfg.lr_sh_dc, f->cfg.lr_sh_rest,
          f->cfg.lr_opacity};
   AdamHyper h{f->cfg.beta1, f->cfg.beta2, f->cfg.epsilon};
-  fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
-      f->P, f->M, f->V, f->G, f->g_mem ? 1 : 0, f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0,
-      f->cfg.sh_degree, f->cam_dev, rb.g2, f->bc_cur, lr, h);
+  const int keep = f->g_mem ? 1 : 0, exact = f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0;
+  if (bf16)
+    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(f->P, f->R16, f->M16, f->V16, f->G, keep,
+                                                         exact, f->cfg.sh_degree, f->cam_dev,
+                                                         rb.g2, f->bc_cur, rb.scalars, lr, h);
+  else
+    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
+        f->P, soa_of(f->P), soa_of(f->M), soa_of(f->V), f->G, keep, exact, f->cfg.sh_degree,
+        f->cam_dev, rb.g2, f->bc_cur, rb.scalars, lr, h);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[7], s));
+  return DS_OK;
+}
+
+// BF16 storage: rewrites the render copy from the masters after the caller
+// changed them (outside the captured graph, on the step's stream).
+static int refresh_render_copy(ds_fitter* f, cudaStream_t s) {
+  if (f->cfg.storage != DS_STORAGE_BF16 || !f->render_dirty) return DS_OK;
+  const size_t blocks = std::min<size_t>((f->floats + kThreads - 1) / kThreads, 148 * 16);
+  to_bf16_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(f->params_mem, f->render_mem, f->floats);
+  DS_CUDA(cudaGetLastError());
+  f->render_dirty = false;
   return DS_OK;
 }
 
@@ -428,6 +558,7 @@ int ds_fitter_default_config(ds_fitter_config* cfg) {
   cfg->storage = DS_STORAGE_FP32;
   cfg->use_graph = 1;
   cfg->grad_mode = ds_default_grad_mode();
+  cfg->schedule = ds::composite_longest_first() ? DS_SCHEDULE_LONGEST_FIRST : DS_SCHEDULE_RASTER;
   return DS_OK;
 }
 
@@ -441,6 +572,7 @@ int ds_fitter_destroy(ds_fitter* f) {
   cudaFree(f->m_mem);
   cudaFree(f->v_mem);
   cudaFree(f->g_mem);
+  cudaFree(f->render_mem);
   cudaFree(f->target);
   cudaFree(f->image);
   cudaFree(f->cam_dev);
@@ -456,8 +588,10 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
   if (cfg->width <= 0 || cfg->height <= 0 || cfg->count <= 0 || cfg->sh_degree < 0 ||
       cfg->sh_degree > 3)
     return DS_ERR_ARG;
-  if (cfg->storage != DS_STORAGE_FP32) return DS_ERR_ARG;
+  if (cfg->storage != DS_STORAGE_FP32 && cfg->storage != DS_STORAGE_BF16) return DS_ERR_ARG;
   if (cfg->grad_mode != DS_GRAD_REFERENCE && cfg->grad_mode != DS_GRAD_EXACT) return DS_ERR_ARG;
+  if (cfg->schedule != DS_SCHEDULE_LONGEST_FIRST && cfg->schedule != DS_SCHEDULE_RASTER)
+    return DS_ERR_ARG;
   ds_fitter* f = new (std::nothrow) ds_fitter();
   if (!f) return DS_ERR_OOM;
   f->cfg = *cfg;
@@ -469,15 +603,26 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
     ds_fitter_destroy(f);
     return code;
   };
+  const bool bf16 = cfg->storage == DS_STORAGE_BF16;
+  const size_t mom_bytes = f->floats * (bf16 ? 2 : 4);
   if ((st = ds::cuda_status(cudaMalloc(&f->params_mem, f->floats * 4)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->m_mem, f->floats * 4)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->v_mem, f->floats * 4)))) return fail(st);
+  if ((st = ds::cuda_status(cudaMalloc(&f->m_mem, mom_bytes)))) return fail(st);
+  if ((st = ds::cuda_status(cudaMalloc(&f->v_mem, mom_bytes)))) return fail(st);
   cudaMemset(f->params_mem, 0, f->floats * 4);
-  cudaMemset(f->m_mem, 0, f->floats * 4);
-  cudaMemset(f->v_mem, 0, f->floats * 4);
+  cudaMemset(f->m_mem, 0, mom_bytes);
+  cudaMemset(f->v_mem, 0, mom_bytes);
   ds::carve(f->params_mem, n, f->bands, f->P);
-  ds::carve(f->m_mem, n, f->bands, f->M);
-  ds::carve(f->v_mem, n, f->bands, f->V);
+  if (bf16) {
+    if ((st = ds::cuda_status(cudaMalloc(&f->render_mem, f->floats * 2)))) return fail(st);
+    cudaMemset(f->render_mem, 0, f->floats * 2);
+    ds::carve_soa(f->render_mem, n, f->bands, f->R16);
+    ds::carve_soa((__nv_bfloat16*)f->m_mem, n, f->bands, f->M16);
+    ds::carve_soa((__nv_bfloat16*)f->v_mem, n, f->bands, f->V16);
+    f->M = f->V = ds_gaussian3d{};  // FP32 views do not exist in this mode
+  } else {
+    ds::carve(f->m_mem, n, f->bands, f->M);
+    ds::carve(f->v_mem, n, f->bands, f->V);
+  }
   if (keep_grads) {
     if ((st = ds::cuda_status(cudaMalloc(&f->g_mem, f->floats * 4)))) return fail(st);
     cudaMemset(f->g_mem, 0, f->floats * 4);
@@ -491,6 +636,7 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
   cudaMemset(f->image, 0, px * 3 * 4);
   if ((st = ds::raster_alloc(f->rb, cfg->width, cfg->height, n, cfg->max_isects))) return fail(st);
   f->rb.grad_mode = cfg->grad_mode;
+  f->rb.schedule = cfg->schedule;
   if ((st = ds::cuda_status(cudaMalloc(&f->cam_dev, sizeof(ds::Camera))))) return fail(st);
   cudaMemset(f->cam_dev, 0, sizeof(ds::Camera));
   // Bias-correction table: bc_k(t) = 1 / (1 - powf(beta_k, t)) on the host, like
@@ -523,6 +669,13 @@ int ds_fitter_create(const ds_fitter_config* cfg, ds_fitter** out) {
 int ds_fitter_params(ds_fitter* f, ds_gaussian3d* out) {
   if (!f || !out) return DS_ERR_ARG;
   *out = f->P;
+  f->render_dirty = true;
+  return DS_OK;
+}
+
+int ds_fitter_params_updated(ds_fitter* f) {
+  if (!f) return DS_ERR_ARG;
+  f->render_dirty = true;
   return DS_OK;
 }
 
@@ -565,6 +718,7 @@ int ds_fitter_step(ds_fitter* f, int n_steps, ds_stream stream) {
     f->graph = g;
     DS_CUDA(cudaGraphInstantiate(&f->exec, f->graph, 0));
   }
+  if (n_steps > 0) DS_TRY(ds::refresh_render_copy(f, s));
   for (int k = 0; k < n_steps; ++k) {
     if (f->exec) {
       DS_CUDA(cudaGraphLaunch(f->exec, s));
@@ -611,6 +765,7 @@ int ds_fitter_profile_step(ds_fitter* f, float* stage_ms, int n_stages, ds_strea
   if (!f->have_target || !f->have_camera) return DS_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
   cudaEvent_t ev[8];
+  DS_TRY(ds::refresh_render_copy(f, s));
   for (int k = 0; k < 8; ++k) DS_CUDA(cudaEventCreate(&ev[k]));
   int st = ds::fitter_enqueue(f, s, ev);
   if (st == DS_OK) st = ds::cuda_status(cudaEventSynchronize(ev[7]));
@@ -637,6 +792,19 @@ int ds_fitter_counters(ds_fitter* f, uint64_t* out, int n) {
   return DS_OK;
 }
 
+int ds_fitter_pair_stats(ds_fitter* f, uint64_t* out, int n, ds_stream stream) {
+  if (!f || !out || n < 2) return DS_ERR_ARG;
+  if (f->host_steps == 0) return DS_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  DS_TRY(ds::raster_composite_count(f->rb, f->image, s));
+  DS_CUDA(cudaStreamSynchronize(s));
+  unsigned long long p[2];
+  DS_CUDA(cudaMemcpy(p, f->rb.scalars->pairs, sizeof(p), cudaMemcpyDeviceToHost));
+  out[0] = p[0];
+  out[1] = p[1];
+  return DS_OK;
+}
+
 // Test hook: a fitter that also writes the Gaussian3D gradients of each step.
 int ds_fitter_create_with_grads(const ds_fitter_config* cfg, ds_fitter** out) {
   return ds_fitter_create_impl(cfg, 1, out);
@@ -651,6 +819,7 @@ int ds_fitter_grads(ds_fitter* f, ds_gaussian3d* out) {
 
 int ds_fitter_moments(ds_fitter* f, ds_gaussian3d* m, ds_gaussian3d* v) {
   if (!f || !m || !v) return DS_ERR_ARG;
+  if (f->cfg.storage != DS_STORAGE_FP32) return DS_ERR_STATE;
   *m = f->M;
   *v = f->V;
   return DS_OK;

@@ -78,7 +78,8 @@ struct DevScalars {
   uint32_t pad[2];
   unsigned long long n_isects_raw;  // unclamped pair count
   float loss;
-  float pad2[3];
+  float pad2;
+  unsigned long long pairs[2];  // counting forward: contributing, tested (pixel, splat) pairs
 };
 
 // ---------------------------------------------------------------------------
@@ -90,6 +91,7 @@ struct RasterBuffers {
   int64_t cap = 0;  // intersection capacity
   int grad_mode = DS_GRAD_REFERENCE;
   int ppt = 2;  // pixels per thread of the composite kernels (1, 2 or 4)
+  int schedule = DS_SCHEDULE_LONGEST_FIRST;  // composite tile order
 
   // per splat
   float4* rec_a = nullptr;
@@ -124,6 +126,7 @@ struct RasterBuffers {
 
   // per tile / pixel
   int2* ranges = nullptr;
+  int32_t* tile_order = nullptr;  // composite schedule: tiles by descending list length
   float* alphas = nullptr;
   int32_t* last_ids = nullptr;
   float* loss_partials = nullptr;  // [tiles]
@@ -138,6 +141,9 @@ int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64
 // Pixels per thread of the composite kernels; DS_COMPOSITE_PPT=1|2|4 overrides
 // the default (a tuning knob: results are identical for every value).
 int composite_default_ppt();
+// Composite CTA schedule: longest tile lists first (default) or raster order
+// (DS_TILE_SCHEDULE=raster).
+bool composite_longest_first();
 int raster_resize(RasterBuffers& rb, int width, int height);
 void raster_free(RasterBuffers& rb);
 
@@ -147,6 +153,11 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
 
 // Composite forward.  When target != nullptr the per-tile squared error is
 // also accumulated and reduced into rb.scalars->loss (L = sum / pixels).
+// Forward that also counts (pixel, splat) pairs into scalars->pairs (which it
+// zeroes first): [0] pairs that contribute (alpha >= 1/255 before the pixel
+// terminates), [1] pairs the kernel evaluates (pixel alive, splat inside the
+// warp's acceptance box).  Outputs are those of raster_composite_forward.
+int raster_composite_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s);
 int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* target,
                              cudaStream_t s);
 // Composite backward into rb.isect_grad.  dL/dpixel is read from grad_rgb, or,

@@ -154,6 +154,69 @@ __global__ void __launch_bounds__(kThreads)
   ranges[t] = a < b ? make_int2((int)a, (int)b) : make_int2(0, 0);
 }
 
+// Longest-first schedule of the composite CTAs: tiles bucketed by their list
+// length (quarter-octave buckets), buckets in descending order.  The heaviest
+// tiles start in the first wave, so they no longer set the kernel's tail.  The
+// order inside a bucket is arbitrary; every tile's result is independent of it.
+constexpr int kOrderBuckets = 128;
+
+__device__ __forceinline__ int work_bucket(int2 r) {
+  const uint32_t len = (uint32_t)max(r.y - r.x, 0);
+  if (len == 0) return 0;
+  const int l = 31 - __clz(len);
+  const uint32_t sub = l >= 2 ? (len >> (l - 2)) & 3u : (len << (2 - l)) & 3u;
+  return min(kOrderBuckets - 1, 1 + 4 * l + (int)sub);
+}
+
+__global__ void __launch_bounds__(1024)
+    tile_order_kernel(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
+  __shared__ uint32_t cnt[kOrderBuckets];
+  __shared__ uint32_t off[kOrderBuckets];
+  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0u;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int rounds = (tiles + (int)blockDim.x - 1) / (int)blockDim.x;
+  for (int r = 0; r < rounds; ++r) {
+    const int t = r * blockDim.x + threadIdx.x;
+    const int b = t < tiles ? work_bucket(ranges[t]) : -1;
+    const uint32_t peers = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[b], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // lane l owns buckets 127-4l .. 124-4l (descending); exclusive scan over lanes
+    uint32_t v[4], s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = cnt[kOrderBuckets - 1 - 4 * lane - k];
+      s += v[k];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    uint32_t run = incl - s;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      off[kOrderBuckets - 1 - 4 * lane - k] = run;
+      run += v[k];
+    }
+  }
+  __syncthreads();
+  for (int r = 0; r < rounds; ++r) {
+    const int t = r * blockDim.x + threadIdx.x;
+    const int b = t < tiles ? work_bucket(ranges[t]) : -1;
+    const uint32_t peers = __match_any_sync(0xffffffffu, b);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(&off[b], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (b >= 0) order[base + __popc(peers & ((1u << lane) - 1u))] = t;
+  }
+}
+
 template <typename T>
 int alloc(T** p, size_t n) {
   *p = nullptr;
@@ -182,6 +245,7 @@ int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64
   rb.max_splats = max_splats;
   rb.cap = cap;
   rb.ppt = composite_default_ppt();
+  rb.schedule = composite_longest_first() ? DS_SCHEDULE_LONGEST_FIRST : DS_SCHEDULE_RASTER;
   const size_t n = (size_t)max_splats;
   DS_TRY(alloc(&rb.rec_a, n));
   DS_TRY(alloc(&rb.rec_b, n));
@@ -218,6 +282,7 @@ int raster_resize(RasterBuffers& rb, int width, int height) {
   if (width <= 0 || height <= 0) return DS_ERR_ARG;
   if (width == rb.width && height == rb.height) return DS_OK;
   release(rb.ranges);
+  release(rb.tile_order);
   release(rb.alphas);
   release(rb.last_ids);
   release(rb.loss_partials);
@@ -229,6 +294,7 @@ int raster_resize(RasterBuffers& rb, int width, int height) {
   if (rb.ntx > 65535 || rb.nty > 65535) return DS_ERR_ARG;
   const size_t px = (size_t)width * height;
   DS_TRY(alloc(&rb.ranges, (size_t)rb.tiles));
+  DS_TRY(alloc(&rb.tile_order, (size_t)rb.tiles));
   DS_TRY(alloc(&rb.alphas, px));
   DS_TRY(alloc(&rb.last_ids, px));
   DS_TRY(alloc(&rb.loss_partials, (size_t)rb.tiles));
@@ -262,6 +328,7 @@ void raster_free(RasterBuffers& rb) {
   release(rb.scan.partials);
   release(rb.scalars);
   release(rb.ranges);
+  release(rb.tile_order);
   release(rb.alphas);
   release(rb.last_ids);
   release(rb.loss_partials);
@@ -315,6 +382,10 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
   ranges_kernel<<<(rb.tiles + kThreads - 1) / kThreads, kThreads, 0, s>>>(
       rb.sorted_tile, &sc->n_isects, rb.tiles, rb.ranges);
   DS_CUDA(cudaGetLastError());
+  if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST) {
+    tile_order_kernel<<<1, 1024, 0, s>>>(rb.ranges, rb.tiles, rb.tile_order);
+    DS_CUDA(cudaGetLastError());
+  }
   if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
   return DS_OK;
 }

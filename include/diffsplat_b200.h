@@ -39,7 +39,11 @@ extern "C" {
 
 /* Storage modes for ds_fitter. */
 #define DS_STORAGE_FP32 0 /* all attributes, SH and Adam moments in FP32 */
-#define DS_STORAGE_BF16 1 /* attributes, SH and Adam moments in BF16; FP32 master weights */
+/* DS_STORAGE_BF16: scale, rotation, SH and opacity are rendered from a BF16
+ * copy of the FP32 master weights (rewritten after every Adam update, round to
+ * nearest); positions stay FP32; Adam m and v are BF16 with stochastic rounding.
+ * Transmittance, blending and gradient sums stay FP32. */
+#define DS_STORAGE_BF16 1
 
 /* Gradient of the compositing backward with respect to alpha.
  * DS_GRAD_REFERENCE reproduces the reference's recurrence
@@ -49,6 +53,11 @@ extern "C" {
  * derivative (matches finite differences). */
 #define DS_GRAD_REFERENCE 0
 #define DS_GRAD_EXACT 1
+
+/* Order in which the composite kernels visit tiles (results do not depend on
+ * it): the longest tile lists first (default), or raster order. */
+#define DS_SCHEDULE_LONGEST_FIRST 0
+#define DS_SCHEDULE_RASTER 1
 
 typedef void *ds_stream; /* cudaStream_t; NULL selects the legacy default stream */
 
@@ -215,12 +224,16 @@ typedef struct ds_fitter_config {
   int32_t storage;   /* DS_STORAGE_FP32 / DS_STORAGE_BF16 */
   int32_t use_graph; /* 1: capture the step into a CUDA graph on first use */
   int32_t grad_mode; /* DS_GRAD_REFERENCE (default) / DS_GRAD_EXACT */
+  int32_t schedule;  /* DS_SCHEDULE_LONGEST_FIRST (default) / DS_SCHEDULE_RASTER */
 } ds_fitter_config;
 
 int ds_fitter_default_config(ds_fitter_config *cfg);
 int ds_fitter_create(const ds_fitter_config *cfg, ds_fitter **out);
 /* Device views of the fitter's FP32 master parameters (write them before the first step). */
 int ds_fitter_params(ds_fitter *f, ds_gaussian3d *out);
+/* Tells the fitter the masters were written through the ds_fitter_params view
+ * (BF16 storage rebuilds its render copy before the next step; FP32: no-op). */
+int ds_fitter_params_updated(ds_fitter *f);
 /* Copies the target image [H*W*3] from a device pointer. */
 int ds_fitter_set_target(ds_fitter *f, const float *target, ds_stream stream);
 /* Camera for the following steps (column-major PV and world camera position, host arrays). */
@@ -251,6 +264,11 @@ int ds_fitter_profile_step(ds_fitter *f, float *stage_ms, int n_stages, ds_strea
 /* out[0] = (tile, splat) pairs, out[1] = visible splats, out[2] = device step
  * count, all of the most recent step (synchronises). */
 int ds_fitter_counters(ds_fitter *f, uint64_t *out, int n);
+/* Re-runs the composite forward of the most recent step with pair counters
+ * (no reference counterpart; measurement only): out[0] = (pixel, splat) pairs
+ * that contribute (alpha >= 1/255 before the pixel terminates), out[1] = pairs
+ * the kernel evaluates.  Rewrites the same image; synchronises. */
+int ds_fitter_pair_stats(ds_fitter *f, uint64_t *out, int n, ds_stream stream);
 int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
 int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
 

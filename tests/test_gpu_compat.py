@@ -42,19 +42,44 @@ def test_reference_grad_check_in_exact_mode(cuda_lib):
     assert max(abs(a - n) for a, n in ref_mode) > 3e-4
 
 
+def _fail_entries(out):
+    """{(field, index): (analytic, numeric, rel_err)} of the checker's FAIL lines;
+    each field's summary line follows its entries."""
+    pending, entries = [], {}
+    for l in out.splitlines():
+        t = l.split()
+        if l.strip().startswith("FAIL ["):
+            f = dict(kv.split("=") for kv in t[2:])
+            pending.append((int(t[1].strip("[]")), float(f["analytic"]), float(f["numeric"]),
+                            float(f["rel_err"])))
+        elif len(t) >= 2 and t[1] in ("PASS", "FAIL"):
+            for idx, a, n, r in pending:
+                entries[(t[0], idx)] = (a, n, r)
+            pending = []
+    return entries
+
+
 def test_reference_grad_check_in_reference_mode_matches_reference_build(cuda_lib):
     """In reference mode the drop-in reproduces the reference's gradients, so the
-    reference's own checker reports failures of the same kind as when it is run
-    on the reference build itself (its alpha-gradient recurrence is not the
-    derivative when splats overlap)."""
+    reference's own checker fails on the same entries as when it runs on the
+    reference build itself (its alpha-gradient recurrence is not the derivative
+    when splats overlap).  Entries within the checker's FP32 noise of its 5%
+    tolerance may flip from run to run (the loss is an atomic FP32 sum in both
+    builds), so only the clear failures (rel_err > 0.1 and |analytic - numeric|
+    > 2e-4) must agree, and the analytic values of common entries must match
+    to the printed precision."""
     mine = ROOT / "oracle" / "_ref" / "grad_check_b200"
     theirs = ROOT / "oracle" / "_ref" / "grad_check_ref"
     if not (mine.exists() and theirs.exists()):
         pytest.skip("reference builds absent")
     a, b = _run(mine, "reference"), _run(theirs, "reference")
-    fails = lambda out: [l.split()[0] for l in out.splitlines() if "FAIL  (" in l]
     assert a.returncode != 0 and b.returncode != 0
-    assert fails(a.stdout) == fails(b.stdout)
+    ea, eb = _fail_entries(a.stdout), _fail_entries(b.stdout)
+    clear = lambda e: {k for k, (x, y, r) in e.items() if r > 0.1 and abs(x - y) > 2e-4}
+    assert clear(ea) <= set(eb) and clear(eb) <= set(ea)
+    assert len(clear(eb)) >= 10
+    for k in set(ea) & set(eb):
+        assert abs(ea[k][0] - eb[k][0]) <= 2e-5, k
 
 
 def test_cpp_image_fitter_smoke(cuda_lib, tmp_path):

@@ -97,3 +97,51 @@ def test_overflow_is_reported(cuda_lib):
     assert code == L.DS_ERR_ISECT_OVERFLOW and flags & 1
     assert np.isfinite(f.params.cpu().numpy()).all()
     f.close()
+
+
+_SCHEDULE_CHILD = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from diffsplat_b200 import api
+from diffsplat_b200.scenes import small_problem
+prob = small_problem(200, 120, 900, seed=6, sh_degree=1)
+f = api.Fitter(prob.width, prob.height, prob.params.shape[1], prob.sh_degree, lrs=prob.lrs,
+               max_isects=1 << 20)
+f.set_params(prob.params)
+f.set_target(torch.tensor(prob.target, device="cuda"))
+f.set_camera(prob.pv, prob.cam)
+f.step(3)
+np.save(sys.argv[2], f.params.cpu().numpy())
+f.close()
+"""
+
+
+def test_tile_schedule_does_not_change_results(cuda_lib, tmp_path):
+    """The composite CTAs run longest tile list first by default; raster order
+    (DS_TILE_SCHEDULE=raster) must give bit-identical parameters."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = str(Path(__file__).resolve().parents[1])
+    out = {}
+    for sched in ("longest-first", "raster"):
+        path = tmp_path / f"{sched}.npy"
+        env = dict(os.environ, DS_TILE_SCHEDULE=sched)
+        r = subprocess.run([sys.executable, "-c", _SCHEDULE_CHILD, root, str(path)], env=env,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[sched] = np.load(path)
+    assert np.array_equal(out["longest-first"].view(np.uint32), out["raster"].view(np.uint32))
+
+
+def test_pair_stats(cuda_lib):
+    prob = small_problem(128, 96, 700, seed=12, sh_degree=0)
+    f = _fitter(prob)
+    f.step(1)
+    img0 = f.image().cpu().numpy().copy()
+    p = f.pair_stats()
+    assert 0 < p["contributing"] <= p["evaluated"]
+    assert p["evaluated"] <= f.counters()["n_isects"] * 256
+    assert np.array_equal(f.image().cpu().numpy(), img0)
+    f.close()

@@ -19,8 +19,12 @@ CASES = ["grad_check_8", "persp_sh0_48x32", "persp_sh1_64x40", "persp_sh3_80x48"
 
 
 def _problem(d) -> FitProblem:
+    """The reference's setCamera forms PV = proj * view (identity view here) on
+    the host, which turns the -0.0 entries of an orthographic proj into +0.0;
+    the C ABI takes that product, so the fixture's matrix gets the same zeros."""
     W, H, deg = (int(x) for x in d["meta"])
-    return FitProblem(W, H, d["params"], d["target"], d["pv"], d["cam"], deg,
+    pv = d["pv"] + np.float32(0.0)
+    return FitProblem(W, H, d["params"], d["target"], pv, d["cam"], deg,
                       tuple(float(x) for x in d["lrs"]))
 
 
