@@ -300,6 +300,66 @@ def profile_run(args):
         sys.exit(1)
 
 
+def run_viewer(args) -> dict:
+    """Viewer-style SH-3 scene: 1M splats, 1920x1080, 16 orbit cameras (fx 1200).
+    Forward-only renders (the SplatRenderer path) and fwd+bwd+Adam fitter steps,
+    FP32 and BF16 storage.  The scene (236 MB of FP32 parameters) exceeds L2."""
+    import torch
+    from diffsplat_b200 import _lib as L
+    from diffsplat_b200 import api
+    from diffsplat_b200.scenes import make_target, orbit_cameras, viewer_scene
+    torch.cuda.set_device(0)
+    W, H, n = 1920, 1080, 1_000_000
+    P = torch.tensor(viewer_scene(n, seed=0), device="cuda")
+    cams = orbit_cameras(16, width=W, height=H, fx=1200.0)
+    tgt = torch.tensor(make_target(W, H, 2000, 7), device="cuda")
+    reps = max(1, args.steps // 100)
+    out = {}
+    for name, storage in (("fp32", L.DS_STORAGE_FP32), ("bf16", L.DS_STORAGE_BF16)):
+        r = api.Renderer(W, H, n, 3, storage=storage)
+        r.set_params(P)
+        for pv, eye in cams[:3]:
+            r.render(pv, eye)
+        torch.cuda.synchronize()
+        evs, isects = [], []
+        with ClockSampler(0) as clk:
+            for _ in range(reps):
+                for pv, eye in cams:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record()
+                    r.render(pv, eye)
+                    b.record()
+                    evs.append((a, b))
+            torch.cuda.synchronize()
+        for pv, eye in cams:
+            r.render(pv, eye)
+            isects.append(r.counts()["n_isects"])
+        code, _ = r.status()
+        r.close()
+        fwd_ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+        f = api.Fitter(W, H, n, 3, storage=storage)
+        f.set_params(P)
+        f.set_target(tgt)
+        f.set_camera(*cams[0])
+        f.step(args.warmup)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        f.step(reps * 10)
+        b.record()
+        torch.cuda.synchronize()
+        step_ms = a.elapsed_time(b) / (reps * 10)
+        stages = f.profile_step()
+        code2, _ = f.status()
+        f.close()
+        out[name] = {"forward_frames_per_s": 1e3 / fwd_ms, "forward_ms": fwd_ms,
+                     "forward_mpix_per_s": W * H / fwd_ms / 1e3,
+                     "fwd_bwd_adam_steps_per_s": 1e3 / step_ms, "fwd_bwd_adam_ms": step_ms,
+                     "stage_ms": stages, "n_isects_per_camera": isects,
+                     "status": max(code, code2), "clocks": clk.summary()}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -310,9 +370,23 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="untimed: warmup + steps eager steps of the same workload with a "
                          "2^22-pair buffer (for ncu captures); prints no JSON line")
+    ap.add_argument("--workload", choices=["fitter", "viewer-sh3"], default="fitter",
+                    help="fitter: the headline 1280x720 / 60000-splat training step; "
+                         "viewer-sh3: 1M-splat SH-3 scene at 1920x1080, forward and fwd+bwd")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.workload == "viewer-sh3":
+        res = run_viewer(args)
+        print(json.dumps({
+            "metric": "viewer-sh3: forward frames/s and fwd+bwd+Adam steps/s",
+            "unit": "frames/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "1M splats on 20 planes/spheres in a radius-10 ball, SH 3, "
+                                   "1920x1080, 16 orbit cameras (radius 15, fx 1200)",
+                       "splats": 1_000_000, "width": 1920, "height": 1080, "sh_degree": 3},
+            "value": res["fp32"]["forward_frames_per_s"], "fp32": res["fp32"],
+            "bf16": res["bf16"]}))
         return
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args.gpus)

@@ -124,6 +124,21 @@ _SIGS = {
     "ds_fitter_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "ds_fitter_pair_stats": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int, _vp]),
     "ds_fitter_params_updated": (C.c_int, [_vp]),
+    "ds_renderer_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int,
+                                     C.POINTER(_vp)]),
+    "ds_renderer_set_params": (C.c_int, [_vp, C.POINTER(Gaussian3D), _vp]),
+    "ds_renderer_set_sh_degree": (C.c_int, [_vp, C.c_int]),
+    "ds_renderer_render": (C.c_int, [_vp, _fp, _fp, _vp]),
+    "ds_renderer_output": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "ds_renderer_resize": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "ds_renderer_counts": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
+    "ds_renderer_status": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
+    "ds_renderer_destroy": (C.c_int, [_vp]),
+    "ds_ply_probe": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    "ds_ply_read": (C.c_int, [C.c_char_p, _fp, C.c_int64, C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int)]),
+    "ds_ply_write": (C.c_int, [C.c_char_p, _fp, C.c_int64, C.c_int]),
+    "ds_normalize_scene": (C.c_int, [_fp, C.c_int64, C.c_float]),
 }
 
 _lib = None

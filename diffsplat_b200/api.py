@@ -336,3 +336,111 @@ class Fitter:
         out = (C.c_uint64 * 2)()
         L.call("ds_fitter_pair_stats", self.h, out, 2, _stream())
         return {"contributing": int(out[0]), "evaluated": int(out[1])}
+
+
+class Renderer:
+    """Owns a ds_renderer: the forward-only SplatRenderer path."""
+
+    def __init__(self, width: int, height: int, max_splats: int, sh_degree: int = 0,
+                 max_isects: int = 0, storage: int = L.DS_STORAGE_FP32):
+        h = C.c_void_p()
+        L.call("ds_renderer_create", width, height, max_splats, sh_degree, max_isects, storage,
+               C.byref(h))
+        self.h = h
+        self.width, self.height, self.sh_degree = width, height, sh_degree
+        self.bands = sh_bands(sh_degree)
+        self._params = None
+
+    def close(self):
+        if self.h:
+            L.call("ds_renderer_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params: torch.Tensor, stream=None) -> None:
+        """params: contiguous float32 CUDA tensor [14 + 3K, n] (kept referenced)."""
+        g = g3_view(params, self.bands)
+        L.call("ds_renderer_set_params", self.h, C.byref(g), _stream(stream))
+        self._params = params
+
+    def set_sh_degree(self, degree: int) -> None:
+        L.call("ds_renderer_set_sh_degree", self.h, degree)
+
+    def render(self, pv, cam_pos, stream=None) -> torch.Tensor:
+        L.call("ds_renderer_render", self.h, L.fptr(pv), L.fptr(cam_pos), _stream(stream))
+        return self.image()
+
+    def image(self) -> torch.Tensor:
+        p = C.c_void_p()
+        L.call("ds_renderer_output", self.h, C.byref(p))
+        return _wrap_device(p.value, (self.height, self.width, 3))
+
+    def resize(self, width: int, height: int) -> None:
+        L.call("ds_renderer_resize", self.h, width, height)
+        self.width, self.height = width, height
+
+    def counts(self) -> dict:
+        out = (C.c_uint64 * 2)()
+        L.call("ds_renderer_counts", self.h, out, 2)
+        return {"visible": int(out[0]), "n_isects": int(out[1])}
+
+    def status(self) -> tuple[int, int]:
+        flags = C.c_uint32()
+        code = L.lib().ds_renderer_status(self.h, C.byref(flags))
+        return code, int(flags.value)
+
+
+# ---- scene I/O (host) --------------------------------------------------------
+
+G3_RECORD = 59  # floats of the reference's host Gaussian3D record
+
+
+def records_to_params(rec: np.ndarray, sh_degree: int) -> np.ndarray:
+    """[n, 59] Gaussian3D records -> [14 + 3K, n] parameter rows (SH rest band-major)."""
+    K = sh_bands(sh_degree)
+    n = rec.shape[0]
+    P = np.zeros((14 + 3 * K, n), np.float32)
+    P[0:13] = rec[:, 0:13].T
+    P[13] = rec[:, 58]
+    P[14:14 + 3 * K] = rec[:, 13:13 + 3 * K].T
+    return P
+
+
+def params_to_records(P: np.ndarray) -> np.ndarray:
+    K = (P.shape[0] - 14) // 3
+    rec = np.zeros((P.shape[1], G3_RECORD), np.float32)
+    rec[:, 0:13] = P[0:13].T
+    rec[:, 58] = P[13]
+    rec[:, 13:13 + 3 * K] = P[14:14 + 3 * K].T
+    return rec
+
+
+def read_ply(path) -> tuple[np.ndarray, int]:
+    """PLYLoader::load: returns ([n, 59] Gaussian3D records, SH degree)."""
+    p = str(path).encode()
+    n, deg = C.c_int64(), C.c_int()
+    L.call("ds_ply_probe", p, C.byref(n), C.byref(deg))
+    rec = np.zeros((n.value, G3_RECORD), np.float32)
+    L.call("ds_ply_read", p, rec.ctypes.data_as(C.POINTER(C.c_float)), n.value, C.byref(n),
+           C.byref(deg))
+    return rec, deg.value
+
+
+def write_ply(path, rec: np.ndarray, sh_num_bands: int = 0) -> None:
+    """PLYSaver::save of [n, 59] Gaussian3D records."""
+    rec = np.ascontiguousarray(rec, np.float32)
+    L.call("ds_ply_write", str(path).encode(), rec.ctypes.data_as(C.POINTER(C.c_float)),
+           rec.shape[0], sh_num_bands)
+
+
+def normalize_scene(rec: np.ndarray, scene_scale: float = 1.0) -> np.ndarray:
+    """SplatUtils::normalizeScene on a copy of [n, 59] records."""
+    out = np.ascontiguousarray(rec, np.float32).copy()
+    L.call("ds_normalize_scene", out.ctypes.data_as(C.POINTER(C.c_float)), out.shape[0],
+           scene_scale)
+    return out

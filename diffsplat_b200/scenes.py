@@ -182,3 +182,63 @@ def psnr_from_ref_loss(loss: float) -> float:
     pixels x 3 (src/layers/mse_loss_layer.cu:31)."""
     mse = max(loss / 3.0, 1e-20)
     return 10.0 * math.log10(1.0 / mse)
+
+
+def viewer_scene(n: int = 1_000_000, seed: int = 0, surfaces: int = 20,
+                 sh_degree: int = 3) -> np.ndarray:
+    """Viewer-style scene: means on `surfaces` random planes and spheres inside a
+    radius-10 ball with sigma = 0.02 jitter, log-scales ~N(-4.5, 0.7), opacity
+    logits ~N(0, 1.5), SH DC ~N(0, 0.5), higher bands ~N(0, 0.05), random
+    rotations.  Field-major float32 [14 + 3K, n]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    K = sh_bands(sh_degree)
+    P = np.zeros((14 + 3 * K, n), np.float32)
+    which = rng.integers(0, surfaces, n)
+    pos = np.zeros((n, 3))
+    for s in range(surfaces):
+        idx = np.nonzero(which == s)[0]
+        m = idx.size
+        c = rng.normal(size=3)
+        c = c / np.linalg.norm(c) * rng.uniform(0.0, 6.0)
+        if s % 2 == 0:  # plane patch through c
+            nrm = rng.normal(size=3)
+            nrm /= np.linalg.norm(nrm)
+            a = np.cross(nrm, [1.0, 0.0, 0.0] if abs(nrm[0]) < 0.9 else [0.0, 1.0, 0.0])
+            a /= np.linalg.norm(a)
+            b = np.cross(nrm, a)
+            half = rng.uniform(1.0, 4.0)
+            uv = rng.uniform(-half, half, (m, 2))
+            pts = c + uv[:, :1] * a + uv[:, 1:] * b
+        else:  # sphere around c
+            r = rng.uniform(0.5, 3.0)
+            d = rng.normal(size=(m, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            pts = c + r * d
+        pts = pts + rng.normal(0.0, 0.02, (m, 3))
+        nrmp = np.linalg.norm(pts, axis=1, keepdims=True)
+        pts = np.where(nrmp > 10.0, pts / nrmp * 10.0, pts)
+        pos[idx] = pts
+    P[0:3] = pos.T
+    P[3:6] = rng.normal(-4.5, 0.7, (3, n))
+    q = rng.normal(0.0, 1.0, (4, n))
+    P[6:10] = q / np.linalg.norm(q, axis=0, keepdims=True)
+    P[10:13] = rng.normal(0.0, 0.5, (3, n))
+    P[13] = rng.normal(0.0, 1.5, n)
+    if K:
+        P[14:] = rng.normal(0.0, 0.05, (3 * K, n))
+    return P
+
+
+def orbit_cameras(count: int = 16, radius: float = 15.0, width: int = 1920, height: int = 1080,
+                  fx: float = 1200.0, near: float = 0.1, far: float = 100.0):
+    """`count` cameras on a horizontal circle of `radius` looking at the origin
+    (GL lookAt + perspective, fovy = 2 atan(height / 2 / fx)): [(pv, eye)]."""
+    fovy = 2.0 * math.atan(height / 2.0 / fx)
+    cams = []
+    for k in range(count):
+        a = 2.0 * math.pi * k / count
+        eye = np.array([radius * math.cos(a), 2.0, radius * math.sin(a)], np.float32)
+        pv = look_at_perspective_pv(eye, [0.0, 0.0, 0.0], [0.0, 1.0, 0.0], fovy, width / height,
+                                    near, far)
+        cams.append((pv, eye))
+    return cams

@@ -272,6 +272,44 @@ int ds_fitter_pair_stats(ds_fitter *f, uint64_t *out, int n, ds_stream stream);
 int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
 int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
 
+/* ---- Forward-only renderer: SplatRenderer (src/pipelines/splat_renderer.h:17-60) ----
+ * render() = GaussActiv -> PerspProject -> TileRasterize forward
+ * (src/pipelines/splat_renderer.cpp:84-91) into an owned [H*W*3] image.
+ * FP32 storage reads the caller's parameter buffers on every render (keep them
+ * alive); BF16 storage converts scale, rotation, SH and opacity into its own
+ * BF16 copy at ds_renderer_set_params (positions stay FP32). */
+typedef struct ds_renderer ds_renderer;
+int ds_renderer_create(int width, int height, int max_splats, int sh_degree, int64_t max_isects,
+                       int storage, ds_renderer **out);
+int ds_renderer_set_params(ds_renderer *r, const ds_gaussian3d *params, ds_stream stream);
+/* setActiveSHDegree: evaluate SH up to `degree` (<= the buffers' degree). */
+int ds_renderer_set_sh_degree(ds_renderer *r, int degree);
+int ds_renderer_render(ds_renderer *r, const float pv[16], const float cam_pos[3],
+                       ds_stream stream);
+int ds_renderer_output(ds_renderer *r, float **rgb);
+int ds_renderer_resize(ds_renderer *r, int width, int height);
+/* out[0] = visible splats, out[1] = (tile, splat) pairs of the last render (synchronises). */
+int ds_renderer_counts(ds_renderer *r, uint64_t *out, int n);
+int ds_renderer_status(ds_renderer *r, uint32_t *flags);
+int ds_renderer_destroy(ds_renderer *r);
+
+/* ---- Scene I/O on the host: PLYLoader / PLYSaver (src/io/ply_io.h:28-57) and
+ * SplatUtils::normalizeScene (src/utils/splat_utils.h) ----
+ * Splats are arrays of the reference's host record Gaussian3D
+ * (src/types/gaussian3d.h:13-21): 59 floats each (pos xyz, log-scale xyz,
+ * quaternion wxyz, SH DC rgb, 45 SH-rest floats channel-first, logit opacity).
+ * Files are binary little-endian 3DGS PLY in the OpenCV frame; y, z and the
+ * quaternion's y, z are negated on read and write (OpenGL frame in memory).
+ * Errors (missing file or property, wrong extension, short file) return DS_ERR_ARG. */
+int ds_ply_probe(const char *path, int64_t *count, int *sh_degree);
+int ds_ply_read(const char *path, float *splats, int64_t capacity, int64_t *count,
+                int *sh_degree);
+/* Writes x y z f_dc_0..2 f_rest_0..(3K-1) opacity scale_0..2 rot_0..3, K = sh_num_bands. */
+int ds_ply_write(const char *path, const float *splats, int64_t count, int sh_num_bands);
+/* Centres the positions on their centroid and scales the largest |coordinate|
+ * to scene_scale, adding log(scale) to the log-scales. */
+int ds_normalize_scene(float *splats, int64_t count, float scene_scale);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -69,3 +69,17 @@ def ref_layers(prob):
 
 def not_culled(S2: np.ndarray) -> np.ndarray:
     return S2[2] != FLT_MAX
+
+
+def bf16_round(x):
+    """FP32 -> BF16 -> FP32, round to nearest even (the BF16 render copy's rounding)."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def render_params(P):
+    """The attributes a BF16-storage forward reads: positions FP32, the rest BF16."""
+    R = bf16_round(P)
+    R[0:3] = P[0:3]
+    return R

@@ -6,23 +6,9 @@ import numpy as np
 import pytest
 
 from diffsplat_b200.scenes import small_problem
-from tests.helpers import rel_err
+from tests.helpers import rel_err, render_params
 
 pytestmark = pytest.mark.gpu
-
-
-def bf16_round(x):
-    """FP32 -> BF16 -> FP32, round to nearest even (the render copy's rounding)."""
-    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
-    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
-    return u.astype(np.uint32).view(np.float32)
-
-
-def render_params(P):
-    """The attributes a BF16-mode forward reads: positions FP32, the rest BF16."""
-    R = bf16_round(P)
-    R[0:3] = P[0:3]
-    return R
 
 
 def _fitter(prob, storage, **kw):
