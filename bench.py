@@ -360,6 +360,76 @@ def run_viewer(args) -> dict:
     return out
 
 
+def run_batch(args) -> dict:
+    """64 uneven fitting instances (sizes from {128^2, 256^2, 512^2, 640x480,
+    1024x768}, 2k-200k splats log-uniform) in one graph-captured step with
+    BF16 storage and autotuned tile size / pixels per thread / CTA schedule,
+    against the same instances fitted one after another by the FP32 fitter."""
+    import torch
+    from diffsplat_b200 import _lib as L
+    from diffsplat_b200 import api, autotune
+    from diffsplat_b200.scenes import batch_problems, psnr_from_ref_loss
+    torch.cuda.set_device(0)
+    probs = batch_problems(64, seed=0)
+    sizes = [(p.width, p.height, p.params.shape[1]) for p in probs]
+    targets = [torch.tensor(p.target, device="cuda") for p in probs]
+    lrs = probs[0].lrs
+
+    def setup(b):
+        for k, p in enumerate(probs):
+            b.set_params(k, p.params)
+            b.set_target(k, targets[k])
+            b.set_camera(k, p.pv, p.cam)
+
+    cap = 1 << 27  # pairs of all 64 instances (about 27M at 32-pixel tiles)
+    best, table = autotune.tune_batch(sizes, setup, lrs=lrs, max_isects=cap)
+    b = api.Batch(sizes, lrs=lrs, max_isects=cap, **best)
+    setup(b)
+    b.step(args.warmup)
+    torch.cuda.synchronize()
+    steps = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        t0.record()
+        b.step(steps)
+        t1.record()
+        torch.cuda.synchronize()
+    batch_ms = t0.elapsed_time(t1)
+    batch_psnr = [psnr_from_ref_loss(x) for x in b.losses()]
+    code, _ = b.status()
+    isects = b.counters()["n_isects"]
+    b.close()
+    # sequential FP32 fitters, same number of steps each
+    seq_ms, seq_psnr = 0.0, []
+    for k, p in enumerate(probs):
+        f = api.Fitter(p.width, p.height, p.params.shape[1], 0, lrs=lrs)
+        f.set_params(p.params)
+        f.set_target(targets[k])
+        f.set_camera(p.pv, p.cam)
+        f.step(args.warmup)
+        torch.cuda.synchronize()
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        f.step(steps)
+        c.record()
+        torch.cuda.synchronize()
+        seq_ms += a.elapsed_time(c)
+        seq_psnr.append(psnr_from_ref_loss(f.loss()))
+        f.close()
+    pixels = sum(w * h for w, h, _ in sizes)
+    dpsnr = [x - y for x, y in zip(batch_psnr, seq_psnr)]
+    return {"instances": len(sizes), "splats": sum(n for _, _, n in sizes), "pixels": pixels,
+            "tuned": best, "tuning_ms_per_step": [[c, ms] for c, ms in table],
+            "batch_steps_per_s": steps / (batch_ms / 1e3),
+            "batch_instance_steps_per_s": len(sizes) * steps / (batch_ms / 1e3),
+            "batch_mpix_per_s": pixels * steps / (batch_ms / 1e3) / 1e6,
+            "sequential_fp32_instance_steps_per_s": len(sizes) * steps / (seq_ms / 1e3),
+            "speedup_vs_sequential": seq_ms / batch_ms,
+            "psnr_batch_bf16": batch_psnr, "psnr_sequential_fp32": seq_psnr,
+            "psnr_delta_min": min(dpsnr), "psnr_delta_mean": sum(dpsnr) / len(dpsnr),
+            "n_isects": isects, "status": code, "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,12 +440,23 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="untimed: warmup + steps eager steps of the same workload with a "
                          "2^22-pair buffer (for ncu captures); prints no JSON line")
-    ap.add_argument("--workload", choices=["fitter", "viewer-sh3"], default="fitter",
+    ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64"], default="fitter",
                     help="fitter: the headline 1280x720 / 60000-splat training step; "
-                         "viewer-sh3: 1M-splat SH-3 scene at 1920x1080, forward and fwd+bwd")
+                         "viewer-sh3: 1M-splat SH-3 scene at 1920x1080, forward and fwd+bwd; "
+                         "batch64: 64 uneven instances in one batched step vs sequential")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.workload == "batch64":
+        res = run_batch(args)
+        print(json.dumps({
+            "metric": "batch64: aggregate instance-steps/s (fwd+bwd+Adam), BF16 batched",
+            "unit": "instance-steps/s", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic", "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "64 instances, sizes {128^2, 256^2, 512^2, 640x480, "
+                                   "1024x768}, 2k-200k splats log-uniform, SH 0"},
+            "value": res["batch_instance_steps_per_s"], **res}))
         return
     if args.workload == "viewer-sh3":
         res = run_viewer(args)

@@ -79,6 +79,19 @@ GAUSSIAN3D_FIELDS = ("pos_x", "pos_y", "pos_z", "scale_x", "scale_y", "scale_z",
 SPLAT3D_FIELDS = tuple(n for n, _ in Splat3D._fields_[:-1])
 SPLAT2D_FIELDS = tuple(n for n, _ in Splat2D._fields_[:-1])
 
+class BatchInstance(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("count", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("instances", C.c_int32), ("sh_degree", C.c_int32), ("max_isects", C.c_int64)] + [
+        (n, C.c_float) for n in ("lr_pos", "lr_scale", "lr_rot", "lr_sh_dc", "lr_sh_rest",
+                                 "lr_opacity", "beta1", "beta2", "epsilon")] + [
+        (n, C.c_int32) for n in ("storage", "use_graph", "grad_mode", "schedule", "tile_size",
+                                 "pixels_per_thread")]
+
+
 _SIGS = {
     "ds_abi_version": (C.c_int, []),
     "ds_status_string": (C.c_char_p, [C.c_int]),
@@ -124,6 +137,21 @@ _SIGS = {
     "ds_fitter_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "ds_fitter_pair_stats": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int, _vp]),
     "ds_fitter_params_updated": (C.c_int, [_vp]),
+    "ds_batch_default_config": (C.c_int, [C.POINTER(BatchConfig)]),
+    "ds_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(BatchInstance),
+                                  C.POINTER(_vp)]),
+    "ds_batch_params": (C.c_int, [_vp, C.POINTER(Gaussian3D)]),
+    "ds_batch_instance_range": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32)]),
+    "ds_batch_params_updated": (C.c_int, [_vp]),
+    "ds_batch_set_target": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "ds_batch_set_camera": (C.c_int, [_vp, C.c_int, _fp, _fp, _vp]),
+    "ds_batch_step": (C.c_int, [_vp, C.c_int, _vp]),
+    "ds_batch_losses": (C.c_int, [_vp, _fp, _vp]),
+    "ds_batch_output": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "ds_batch_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
+    "ds_batch_status": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
+    "ds_batch_destroy": (C.c_int, [_vp]),
     "ds_renderer_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int,
                                      C.POINTER(_vp)]),
     "ds_renderer_set_params": (C.c_int, [_vp, C.POINTER(Gaussian3D), _vp]),

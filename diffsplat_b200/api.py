@@ -444,3 +444,94 @@ def normalize_scene(rec: np.ndarray, scene_scale: float = 1.0) -> np.ndarray:
     L.call("ds_normalize_scene", out.ctypes.data_as(C.POINTER(C.c_float)), out.shape[0],
            scene_scale)
     return out
+
+
+class Batch:
+    """Owns a ds_batch: many independent fitting instances stepped together.
+
+    sizes: [(width, height, splat count)] per instance."""
+
+    def __init__(self, sizes, sh_degree: int = 0, lrs=None, max_isects: int = 0,
+                 storage: int = L.DS_STORAGE_BF16, tile_size: int = 16, ppt: int = 1,
+                 schedule: int = L.DS_SCHEDULE_LONGEST_FIRST, use_graph: bool = True,
+                 grad_mode: int = L.DS_GRAD_REFERENCE, betas=(0.9, 0.999), eps: float = 1e-8):
+        cfg = L.BatchConfig()
+        L.call("ds_batch_default_config", C.byref(cfg))
+        cfg.instances, cfg.sh_degree, cfg.max_isects = len(sizes), sh_degree, max_isects
+        if lrs is not None:
+            (cfg.lr_pos, cfg.lr_scale, cfg.lr_rot, cfg.lr_sh_dc, cfg.lr_sh_rest,
+             cfg.lr_opacity) = lrs
+        cfg.beta1, cfg.beta2 = betas
+        cfg.epsilon = eps
+        cfg.storage, cfg.use_graph, cfg.grad_mode = storage, 1 if use_graph else 0, grad_mode
+        cfg.schedule, cfg.tile_size, cfg.pixels_per_thread = schedule, tile_size, ppt
+        inst = (L.BatchInstance * len(sizes))()
+        for k, (w, h, n) in enumerate(sizes):
+            inst[k].width, inst[k].height, inst[k].count = w, h, n
+        h = C.c_void_p()
+        L.call("ds_batch_create", C.byref(cfg), inst, C.byref(h))
+        self.h = h
+        self.sizes = [tuple(s) for s in sizes]
+        self.sh_degree = sh_degree
+        self.bands = sh_bands(sh_degree)
+        g = L.Gaussian3D()
+        L.call("ds_batch_params", self.h, C.byref(g))
+        self.params = _wrap_device(g.pos_x, (14 + 3 * self.bands, g.count))
+        self.ranges = []
+        for k in range(len(sizes)):
+            a, n = C.c_int32(), C.c_int32()
+            L.call("ds_batch_instance_range", self.h, k, C.byref(a), C.byref(n))
+            self.ranges.append((a.value, n.value))
+
+    def close(self):
+        if self.h:
+            L.call("ds_batch_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def instance_params(self, k: int) -> torch.Tensor:
+        a, n = self.ranges[k]
+        return self.params[:, a:a + n]
+
+    def set_params(self, k: int, params) -> None:
+        a, n = self.ranges[k]
+        self.params[:, a:a + n].copy_(torch.as_tensor(params, device="cuda"))
+        L.call("ds_batch_params_updated", self.h)
+
+    def set_target(self, k: int, target: torch.Tensor, stream=None) -> None:
+        target = target.contiguous()
+        L.call("ds_batch_set_target", self.h, k, target.data_ptr(), _stream(stream))
+        torch.cuda.current_stream().synchronize()
+
+    def set_camera(self, k: int, pv, cam_pos, stream=None) -> None:
+        L.call("ds_batch_set_camera", self.h, k, L.fptr(pv), L.fptr(cam_pos), _stream(stream))
+
+    def step(self, n: int = 1, stream=None) -> None:
+        L.call("ds_batch_step", self.h, n, _stream(stream))
+
+    def losses(self, stream=None) -> np.ndarray:
+        out = np.zeros(len(self.sizes), np.float32)
+        L.call("ds_batch_losses", self.h, out.ctypes.data_as(C.POINTER(C.c_float)),
+               _stream(stream))
+        return out
+
+    def image(self, k: int) -> torch.Tensor:
+        p = C.c_void_p()
+        L.call("ds_batch_output", self.h, k, C.byref(p))
+        w, h, _ = self.sizes[k]
+        return _wrap_device(p.value, (h, w, 3))
+
+    def counters(self) -> dict:
+        out = (C.c_uint64 * 3)()
+        L.call("ds_batch_counters", self.h, out, 3)
+        return {"n_isects": int(out[0]), "visible": int(out[1]), "step": int(out[2])}
+
+    def status(self) -> tuple[int, int]:
+        flags = C.c_uint32()
+        code = L.lib().ds_batch_status(self.h, C.byref(flags))
+        return code, int(flags.value)

@@ -271,6 +271,7 @@ __device__ __forceinline__ float conic_dist2(float dx, float dy, float a, float 
   return __fmaf_rn(__fmul_rn(dy, dy), c, __fmaf_rn(__fmul_rn(dx, dx), a, __fmul_rn(t2, b)));
 }
 
+template <int TS = kTile>
 __device__ __forceinline__ bool tile_rect(float x, float y, float z, float cxx, float cxy, float cyy,
                                           int width, int height, int ntx, int nty, TileRect& r) {
   if (!(fabsf(x) <= 1.0f && fabsf(y) <= 1.0f && fabsf(z) <= 1.0f)) return false;
@@ -282,8 +283,8 @@ __device__ __forceinline__ bool tile_rect(float x, float y, float z, float cxx, 
   if (!(fmaxf(extent_x, extent_y) * 2.f >= pixel_ndc)) return false;
   float min_x = x - extent_x, max_x = x + extent_x;
   float min_y = y - extent_y, max_y = y + extent_y;
-  const float fx = (float)width / kTile;
-  const float fy = (float)height / kTile;
+  const float fx = (float)width / TS;
+  const float fy = (float)height / TS;
   r.x0 = max((int)floorf((min_x + 1.f) * 0.5f * fx), 0);
   r.x1 = min((int)floorf((max_x + 1.f) * 0.5f * fx), ntx - 1);
   r.y0 = max((int)floorf((1.f - max_y) * 0.5f * fy), 0);

@@ -1,4 +1,4 @@
-// Front-to-back compositing of one 16x16 tile per CTA and its backward.
+// Front-to-back compositing of one tile per CTA and its backward.
 //
 // Semantics: src/layers/tile_rasterize_layer.cu:192-309 (forward) and
 // :356-578 (backward): NDC pixel centres, conic from Cov2D, sigma < 0 skip,
@@ -7,13 +7,19 @@
 // the last contributor, backward by reverse traversal with
 // T_before = T / max(1 - alpha, 1e-6).
 //
-// Layout: each thread owns PPT pixels of one column (PPT = 1, 2 or 4); a warp
-// covers a BW x BH block (8x4, 8x8 or 16x8 pixels) and tests each splat's
-// conservative acceptance box against that block once, so the shared-memory
-// reads, the culling test and (backward) the warp reduction are shared by
-// 32 * PPT pixels.  The backward keeps one gradient partial per warp and splat
-// in shared memory and sums the warps in a fixed order: gradients are
-// deterministic run to run.
+// Layout: tiles are TS x TS pixels (16, the reference's TILE_SIZE; batches may
+// use 8 or 32); each thread owns PPT pixels of one column (PPT = 1, 2 or 4); a
+// warp covers a BW x BH block (8x4, 8x8 or 16x8 pixels).  When a batch of
+// splats is staged in shared memory, each splat's acceptance box is tested
+// once against every warp's block; each warp then walks only its own hits
+// (ballot words of the per-splat warp masks), so shared-memory reads and
+// (backward) the warp reduction are shared by 32 * PPT pixels and misses cost
+// nothing in the inner loop.  The backward keeps one gradient partial per warp
+// and splat in shared memory and sums the warps in a fixed order: gradients
+// are deterministic run to run.
+//
+// Batch mode (kBatch): tile indices are batch-wide; tile_inst / geom give each
+// tile's instance, image size, tile grid and first pixel.
 #include <stdlib.h>
 #include <string.h>
 
@@ -26,16 +32,33 @@ namespace {
 
 constexpr int kFwdBatch = 256;  // splats staged in shared memory per forward batch
 
-template <int PPT>
+template <int PPT, int TS>
 struct Lay {
-  static constexpr int kThreads = kTilePixels / PPT;
+  static constexpr int kThreads = TS * TS / PPT;
   static constexpr int kWarps = kThreads / 32;
   static constexpr int BW = PPT == 4 ? 16 : 8;  // warp block width
   static constexpr int BH = 32 * PPT / BW;      // warp block height
   static constexpr int kLaneRows = 32 / BW;     // rows between a thread's pixels
-  static constexpr int kWarpsX = kTile / BW;
-  static constexpr int kBwdBatch = 64 * PPT;    // keeps the per-warp partials at 18 KB
+  static constexpr int kWarpsX = TS / BW;
+  // backward batch: the per-warp partials (kWarps x kBwdBatch x 36 B) stay at 18 KB
+  static constexpr int kBwdBatch = 512 / kWarps < 256 ? 512 / kWarps : 256;
+  static_assert(kThreads % 32 == 0 && BW <= TS && kWarps <= 32, "unsupported tile layout");
 };
+
+// Where a tile lies: its image size, its tile grid, its index in that grid and
+// the first pixel of its image in the pixel arrays.
+struct TileGeo {
+  int W, H, ntx, local, pix_off;
+};
+
+template <bool kBatch>
+__device__ __forceinline__ TileGeo tile_geo(int tile, int W, int H, int ntx,
+                                            const uint16_t* __restrict__ tile_inst,
+                                            const InstGeom* __restrict__ geom) {
+  if (!kBatch) return TileGeo{W, H, ntx, tile, 0};
+  const InstGeom g = geom[tile_inst[tile]];
+  return TileGeo{g.width, g.height, g.ntx, tile - g.tile_off, g.pix_off};
+}
 
 template <int PPT>
 struct Pixels {
@@ -47,20 +70,20 @@ struct Pixels {
   float wx_lo, wx_hi, wy_lo, wy_hi;  // extremes of the warp's pixel centres (NDC)
 };
 
-template <int PPT>
+template <int PPT, int TS>
 __device__ __forceinline__ Pixels<PPT> pixels(int tile, int ntx, int W, int H) {
-  using Lc = Lay<PPT>;
+  using Lc = Lay<PPT, TS>;
   Pixels<PPT> m;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int trow = tile / ntx, tcol = tile - trow * ntx;
   const int lx = lane % Lc::BW, ly = lane / Lc::BW;
   const int wx = w % Lc::kWarpsX, wy = w / Lc::kWarpsX;
-  m.j = tcol * kTile + wx * Lc::BW + lx;
+  m.j = tcol * TS + wx * Lc::BW + lx;
   m.px = 2.f * (m.j + 0.5f) / W - 1.f;
   float yl = 3.0e38f, yh = -3.0e38f;
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
-    m.i[k] = trow * kTile + wy * Lc::BH + ly + k * Lc::kLaneRows;
+    m.i[k] = trow * TS + wy * Lc::BH + ly + k * Lc::kLaneRows;
     m.inside[k] = m.i[k] < H && m.j < W;
     m.py[k] = 1.f - 2.f * (m.i[k] + 0.5f) / H;
     yl = fminf(yl, m.py[k]);
@@ -96,16 +119,17 @@ __device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4* box
   return mk;
 }
 
-template <int PPT, bool kLoss, bool kCount = false>
-__global__ void __launch_bounds__(Lay<PPT>::kThreads)
+template <int PPT, int TS, bool kLoss, bool kCount, bool kBatch>
+__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
     composite_fwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const uint32_t* __restrict__ sorted_splat,
                          const int2* __restrict__ ranges, const int32_t* __restrict__ order,
                          float* __restrict__ out_rgb, float* __restrict__ out_alpha,
-                         int32_t* __restrict__ last_ids, int W, int H, int ntx,
+                         int32_t* __restrict__ last_ids, int W_, int H_, int ntx_,
+                         const uint16_t* __restrict__ tile_inst, const InstGeom* __restrict__ geom,
                          const float* __restrict__ target, float* __restrict__ loss_partials,
                          DevScalars* __restrict__ sc) {
-  using Lc = Lay<PPT>;
+  using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
   constexpr int NW = Lc::kWarps;
   __shared__ float4 sA[kFwdBatch], sB[kFwdBatch], sC[kFwdBatch];
@@ -114,7 +138,9 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   __shared__ float red[NW];
   __shared__ bool last;
   const int tile = order ? order[blockIdx.x] : (int)blockIdx.x;
-  const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
+  const TileGeo tg = tile_geo<kBatch>(tile, W_, H_, ntx_, tile_inst, geom);
+  const int W = tg.W, H = tg.H;
+  const Pixels<PPT> m = pixels<PPT, TS>(tg.local, tg.ntx, W, H);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
   const int2 range = ranges[tile];
@@ -206,7 +232,7 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     if (!m.inside[k]) continue;
-    const int pix = m.i[k] * W + m.j;
+    const int pix = tg.pix_off + m.i[k] * W + m.j;
     out_rgb[pix * 3 + 0] = Cr[k];
     out_rgb[pix * 3 + 1] = Cg[k];
     out_rgb[pix * 3 + 2] = Cb[k];
@@ -228,11 +254,14 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
       float s = 0.f;
       for (int k = 0; k < Lc::kWarps; ++k) s += red[k];
       loss_partials[tile] = s;
-      __threadfence();
-      last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+      if (!kBatch) {
+        __threadfence();
+        last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+      }
     }
     __syncthreads();
-    if (last) {
+    // Batches sum their per-instance losses in batch_loss_kernel instead.
+    if (!kBatch && last) {
       // The last CTA to finish sums the per-tile partials in tile order.
       __threadfence();
       float s = 0.f;
@@ -251,8 +280,8 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   }
 }
 
-template <int PPT, bool kFusedLoss, bool kExact>
-__global__ void __launch_bounds__(Lay<PPT>::kThreads)
+template <int PPT, int TS, bool kFusedLoss, bool kExact, bool kBatch>
+__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
     composite_bwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const float* __restrict__ ridet,
                          const uint32_t* __restrict__ sorted_splat,
@@ -260,8 +289,10 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
                          const int32_t* __restrict__ order, const float* __restrict__ alphas,
                          const int32_t* __restrict__ last_ids,
                          const float* __restrict__ grad_or_image, const float* __restrict__ target,
-                         float* __restrict__ isect_grad, int W, int H, int ntx) {
-  using Lc = Lay<PPT>;
+                         float* __restrict__ isect_grad, int W_, int H_, int ntx_,
+                         const uint16_t* __restrict__ tile_inst,
+                         const InstGeom* __restrict__ geom) {
+  using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
   constexpr int NW = Lc::kWarps;
   constexpr int B = Lc::kBwdBatch;
@@ -274,7 +305,9 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   const int2 range = ranges[tile];
   const int start = range.x, end = range.y;
   if (end <= start) return;
-  const Pixels<PPT> m = pixels<PPT>(tile, ntx, W, H);
+  const TileGeo tg = tile_geo<kBatch>(tile, W_, H_, ntx_, tile_inst, geom);
+  const int W = tg.W, H = tg.H;
+  const Pixels<PPT> m = pixels<PPT, TS>(tg.local, tg.ntx, W, H);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
   float T[PPT], gr[PPT], gg[PPT], gb[PPT], accr[PPT], accg[PPT], accb[PPT];
@@ -282,7 +315,7 @@ __global__ void __launch_bounds__(Lay<PPT>::kThreads)
   int32_t my_final = -1;
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
-    const int pix = min(m.i[k] * W + m.j, W * H - 1);
+    const int pix = tg.pix_off + min(m.i[k] * W + m.j, W * H - 1);
     T[k] = 1.f - alphas[pix];
     fin[k] = m.inside[k] ? last_ids[pix] : -1;
     my_final = max(my_final, fin[k]);
@@ -411,39 +444,35 @@ const int32_t* schedule(const RasterBuffers& rb) {
   return rb.schedule == DS_SCHEDULE_LONGEST_FIRST ? rb.tile_order : nullptr;
 }
 
-template <int PPT>
-void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, cudaStream_t s) {
-  constexpr int NT = Lay<PPT>::kThreads;
+template <int PPT, int TS, bool kBatch>
+void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, bool count,
+                cudaStream_t s) {
+  constexpr int NT = Lay<PPT, TS>::kThreads;
   const int32_t* order = schedule(rb);
-  if (target)
-    composite_fwd_kernel<PPT, true><<<rb.tiles, NT, 0, s>>>(
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,
-        rb.last_ids, rb.width, rb.height, rb.ntx, target, rb.loss_partials, rb.scalars);
-  else
-    composite_fwd_kernel<PPT, false><<<rb.tiles, NT, 0, s>>>(
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,
-        rb.last_ids, rb.width, rb.height, rb.ntx, nullptr, nullptr, rb.scalars);
+#define DS_FWD(L, C)                                                                         \
+  composite_fwd_kernel<PPT, TS, L, C, kBatch><<<rb.tiles, NT, 0, s>>>(                       \
+      rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,   \
+      rb.last_ids, rb.width, rb.height, rb.ntx, rb.tile_inst, rb.geom, L ? target : nullptr, \
+      L ? rb.loss_partials : nullptr, rb.scalars)
+  if (count) DS_FWD(false, true);
+  else if (target) DS_FWD(true, false);
+  else DS_FWD(false, false);
+#undef DS_FWD
 }
 
-template <int PPT>
-void launch_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
-  composite_fwd_kernel<PPT, false, true><<<rb.tiles, Lay<PPT>::kThreads, 0, s>>>(
-      rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, schedule(rb), out_rgb,
-      rb.alphas, rb.last_ids, rb.width, rb.height, rb.ntx, nullptr, nullptr, rb.scalars);
-}
-
-template <int PPT>
+template <int PPT, int TS, bool kBatch>
 void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, const float* target,
                 cudaStream_t s) {
-  constexpr int NT = Lay<PPT>::kThreads;
+  constexpr int NT = Lay<PPT, TS>::kThreads;
   const float* g = grad_rgb ? grad_rgb : image;
   const float* t = grad_rgb ? nullptr : target;
   const bool exact = rb.grad_mode == DS_GRAD_EXACT;
   const int32_t* order = schedule(rb);
 #define DS_BWD(F, E)                                                                         \
-  composite_bwd_kernel<PPT, F, E><<<rb.tiles, NT, 0, s>>>(                                   \
+  composite_bwd_kernel<PPT, TS, F, E, kBatch><<<rb.tiles, NT, 0, s>>>(                       \
       rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit, rb.ranges, \
-      order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx)
+      order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx,       \
+      rb.tile_inst, rb.geom)
   if (grad_rgb) {
     if (exact) DS_BWD(false, true);
     else DS_BWD(false, false);
@@ -452,6 +481,58 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
     else DS_BWD(true, false);
   }
 #undef DS_BWD
+}
+
+struct FwdOp {
+  RasterBuffers& rb;
+  float* out_rgb;
+  const float* target;
+  bool count;
+  cudaStream_t s;
+  template <int P, int T, bool B>
+  void run() const {
+    launch_fwd<P, T, B>(rb, out_rgb, target, count, s);
+  }
+};
+
+struct BwdOp {
+  RasterBuffers& rb;
+  const float* image;
+  const float* grad_rgb;
+  const float* target;
+  cudaStream_t s;
+  template <int P, int T, bool B>
+  void run() const {
+    launch_bwd<P, T, B>(rb, image, grad_rgb, target, s);
+  }
+};
+
+// Single instance: 16x16 tiles, PPT 1, 2 or 4.  Batch: tiles of 8, 16 or 32
+// pixels with PPT 1 or 2.
+template <class F>
+int dispatch(const RasterBuffers& rb, const F& f) {
+  if (!rb.geom) {
+    switch (rb.ppt) {
+      case 4: f.template run<4, 16, false>(); return DS_OK;
+      case 2: f.template run<2, 16, false>(); return DS_OK;
+      default: f.template run<1, 16, false>(); return DS_OK;
+    }
+  }
+  const bool two = rb.ppt == 2;
+  switch (rb.tile_size) {
+    case 8:
+      if (two) f.template run<2, 8, true>();
+      else f.template run<1, 8, true>();
+      return DS_OK;
+    case 32:
+      if (two) f.template run<2, 32, true>();
+      else f.template run<1, 32, true>();
+      return DS_OK;
+    default:
+      if (two) f.template run<2, 16, true>();
+      else f.template run<1, 16, true>();
+      return DS_OK;
+  }
 }
 
 }  // namespace
@@ -477,31 +558,19 @@ bool composite_longest_first() {
 
 int raster_composite_forward(RasterBuffers& rb, float* out_rgb, const float* target,
                              cudaStream_t s) {
-  switch (rb.ppt) {
-    case 4: launch_fwd<4>(rb, out_rgb, target, s); break;
-    case 2: launch_fwd<2>(rb, out_rgb, target, s); break;
-    default: launch_fwd<1>(rb, out_rgb, target, s); break;
-  }
+  dispatch(rb, FwdOp{rb, out_rgb, target, false, s});
   return cuda_status(cudaGetLastError());
 }
 
 int raster_composite_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
   DS_CUDA(cudaMemsetAsync(rb.scalars->pairs, 0, sizeof(rb.scalars->pairs), s));
-  switch (rb.ppt) {
-    case 4: launch_count<4>(rb, out_rgb, s); break;
-    case 2: launch_count<2>(rb, out_rgb, s); break;
-    default: launch_count<1>(rb, out_rgb, s); break;
-  }
+  dispatch(rb, FwdOp{rb, out_rgb, nullptr, true, s});
   return cuda_status(cudaGetLastError());
 }
 
 int raster_composite_backward(RasterBuffers& rb, const float* image, const float* grad_rgb,
                               const float* target, cudaStream_t s) {
-  switch (rb.ppt) {
-    case 4: launch_bwd<4>(rb, image, grad_rgb, target, s); break;
-    case 2: launch_bwd<2>(rb, image, grad_rgb, target, s); break;
-    default: launch_bwd<1>(rb, image, grad_rgb, target, s); break;
-  }
+  dispatch(rb, BwdOp{rb, image, grad_rgb, target, s});
   return cuda_status(cudaGetLastError());
 }
 

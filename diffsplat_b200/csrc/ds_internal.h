@@ -85,6 +85,13 @@ struct DevScalars {
 // ---------------------------------------------------------------------------
 // Rasterizer state (ds_raster.cu), shared by the layer API and the fitter.
 // ---------------------------------------------------------------------------
+// One fitting instance of a batch: its image, its tile grid and where its
+// tiles and pixels start in the batch-wide tile and pixel arrays.
+struct InstGeom {
+  int width, height, ntx, nty;
+  int tile_off, pix_off, splat_off, count;
+};
+
 struct RasterBuffers {
   int width = 0, height = 0, ntx = 0, nty = 0, tiles = 0;
   int max_splats = 0;
@@ -92,6 +99,15 @@ struct RasterBuffers {
   int grad_mode = DS_GRAD_REFERENCE;
   int ppt = 2;  // pixels per thread of the composite kernels (1, 2 or 4)
   int schedule = DS_SCHEDULE_LONGEST_FIRST;  // composite tile order
+  int tile_size = 16;  // pixels per tile edge: 16 (reference); batches may use 8 or 32
+
+  // Batch mode (several independent instances in one set of buffers): set
+  // together, null for a single instance.  Tiles and pixels are the
+  // concatenation of the instances' grids and images.
+  const uint16_t* inst_of_splat = nullptr;  // [max_splats]
+  const uint16_t* tile_inst = nullptr;      // [tiles]
+  const InstGeom* geom = nullptr;           // [instances]
+  int instances = 0;
 
   // per splat
   float4* rec_a = nullptr;
@@ -145,6 +161,11 @@ int composite_default_ppt();
 // (DS_TILE_SCHEDULE=raster).
 bool composite_longest_first();
 int raster_resize(RasterBuffers& rb, int width, int height);
+// Batch-mode allocation: `tiles` tiles of tile_size^2 pixels over `pixels`
+// pixels in all (the concatenated instance grids); the geometry arrays are set
+// by the caller.
+int raster_alloc_batch(RasterBuffers& rb, int64_t pixels, int tiles, int tile_size,
+                       int max_splats, int64_t cap);
 void raster_free(RasterBuffers& rb);
 
 // Everything after the per-splat records exist: depth sort, emission, tile

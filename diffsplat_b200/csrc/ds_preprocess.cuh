@@ -51,26 +51,43 @@ Soa<float> soa_of(const ds_gaussian3d& g) {
 
 // Preprocess of one step: positions from the FP32 masters P, every other
 // attribute from R (P itself in FP32 storage, the BF16 render copy otherwise).
-template <typename T>
+//
+// Batch mode (kBatch): splat i belongs to instance inst_of_splat[i], whose
+// camera is camp[inst] and whose image and tile grid (TS-pixel tiles) are
+// geom[inst]; W, H, ntx, nty are then ignored.
+template <typename T, int TS = kTile, bool kBatch = false>
 __global__ void __launch_bounds__(kPreThreads)
     fit_preprocess_kernel(ds_gaussian3d P, Soa<T> R, int degree, const Camera* __restrict__ camp,
                           int W, int H, int ntx, int nty, float4* __restrict__ ra,
                           float4* __restrict__ rb, float4* __restrict__ rc,
                           float* __restrict__ ridet, ushort4* __restrict__ rect,
                           uint32_t* __restrict__ counts, uint32_t* __restrict__ depth_keys,
-                          DevScalars* __restrict__ sc) {
+                          DevScalars* __restrict__ sc,
+                          const uint16_t* __restrict__ inst_of_splat = nullptr,
+                          const InstGeom* __restrict__ geom = nullptr) {
   __shared__ Mat4 sP;
   __shared__ float sCam[3];
-  if (threadIdx.x < 16) sP.m[threadIdx.x] = camp->pv[threadIdx.x];
-  if (threadIdx.x < 3) sCam[threadIdx.x] = camp->cam[threadIdx.x];
+  if (!kBatch) {
+    if (threadIdx.x < 16) sP.m[threadIdx.x] = camp->pv[threadIdx.x];
+    if (threadIdx.x < 3) sCam[threadIdx.x] = camp->cam[threadIdx.x];
+  }
   __syncthreads();
   const int n = P.count;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool vis = false;
   if (i < n) {
+    const Camera* cam_i = camp;
+    if (kBatch) {
+      const int inst = inst_of_splat[i];
+      const InstGeom g = geom[inst];
+      cam_i = camp + inst;
+      W = g.width, H = g.height, ntx = g.ntx, nty = g.nty;
+    }
+    const Mat4& PV = kBatch ? *reinterpret_cast<const Mat4*>(cam_i->pv) : sP;
+    const float* eye = kBatch ? cam_i->cam : sCam;
     const float px = P.pos_x[i], py = P.pos_y[i], pz = P.pos_z[i];
     float clip_x, clip_y, clip_z, clip_w;
-    project_jacobian(sP, px, py, pz, clip_x, clip_y, clip_z, clip_w);
+    project_jacobian(PV, px, py, pz, clip_x, clip_y, clip_z, clip_w);
     TileRect r;
     float ndc_x = 0.f, ndc_y = 0.f;
     Cov2 c2 = {0.f, 0.f, 0.f};
@@ -84,11 +101,11 @@ __global__ void __launch_bounds__(kPreThreads)
       ndc_x = clip_x * inv_w;
       ndc_y = clip_y * inv_w;
       const float ndc_z = clip_z * inv_w;
-      Jac2 J = jacobian(sP, clip_x, clip_y, clip_w, inv_w2);
+      Jac2 J = jacobian(PV, clip_x, clip_y, clip_w, inv_w2);
       c2 = cov2_from(J, c3.xx, c3.xy, c3.xz, c3.yy, c3.yz, c3.zz);
-      vis = tile_rect(ndc_x, ndc_y, ndc_z, c2.xx, c2.xy, c2.yy, W, H, ntx, nty, r);
+      vis = tile_rect<TS>(ndc_x, ndc_y, ndc_z, c2.xx, c2.xy, c2.yy, W, H, ntx, nty, r);
       if (vis) {
-        float3 v = dir_to_camera(sCam[0], sCam[1], sCam[2], px, py, pz);
+        float3 v = dir_to_camera(eye[0], eye[1], eye[2], px, py, pz);
         const T* no = nullptr;
         const float cr = clamp01(
             sh_channel(ldv(R.sh_dc_r[i]), degree > 0 ? R.sh_rest_r + i : no, n, degree, v) + 0.5f);

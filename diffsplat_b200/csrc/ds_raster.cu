@@ -65,9 +65,11 @@ __global__ void __launch_bounds__(kThreads)
     emit_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ counts,
                 const unsigned long long* __restrict__ offsets, const ushort4* __restrict__ rect,
                 int n, int ntx, uint32_t cap, uint32_t* __restrict__ tile_keys,
-                uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start) {
+                uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start,
+                const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom) {
   // One warp per splat in depth order; lanes write its tiles (row-major over
-  // the rectangle) to consecutive emission slots.
+  // the rectangle) to consecutive emission slots.  In a batch the tile id is
+  // batch-wide: the instance's first tile plus its row-major tile index.
   const int p = (int)((blockIdx.x * (unsigned)kThreads + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (p >= n) return;
@@ -82,9 +84,15 @@ __global__ void __launch_bounds__(kThreads)
   unsigned long long end = off + c;
   if (end > cap) end = cap;
   const uint32_t m = (uint32_t)(end - off);
+  uint32_t base = 0, pitch = (uint32_t)ntx;
+  if (geom) {
+    const InstGeom g = geom[inst_of_splat[i]];
+    base = (uint32_t)g.tile_off;
+    pitch = (uint32_t)g.ntx;
+  }
   for (uint32_t k = lane; k < m; k += 32) {
     const uint32_t ty = r.z + k / w, tx = r.x + k % w;
-    tile_keys[off + k] = ty * (uint32_t)ntx + tx;
+    tile_keys[off + k] = base + ty * pitch + tx;
     emit_splat[off + k] = i;
   }
 }
@@ -238,8 +246,7 @@ int ceil_log2(int x) {
 
 }  // namespace
 
-int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap) {
-  if (width <= 0 || height <= 0 || max_splats < 0) return DS_ERR_ARG;
+static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   if (cap <= 0) cap = (int64_t)1 << 25;
   if (cap > ((int64_t)1 << 31)) return DS_ERR_ARG;
   rb.max_splats = max_splats;
@@ -275,7 +282,33 @@ int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64
   DS_CUDA(cudaMemset(rb.scalars, 0, sizeof(DevScalars)));
   // Splats that are never visible keep count 0 until the first forward writes them.
   DS_CUDA(cudaMemset(rb.counts, 0, n * sizeof(uint32_t) + (n == 0 ? 4 : 0)));
+  return DS_OK;
+}
+
+int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap) {
+  if (width <= 0 || height <= 0 || max_splats < 0) return DS_ERR_ARG;
+  DS_TRY(raster_alloc_splats(rb, max_splats, cap));
   return raster_resize(rb, width, height);
+}
+
+int raster_alloc_batch(RasterBuffers& rb, int64_t pixels, int tiles, int tile_size,
+                       int max_splats, int64_t cap) {
+  if (pixels <= 0 || tiles <= 0 || max_splats < 0) return DS_ERR_ARG;
+  if (tile_size != 8 && tile_size != 16 && tile_size != 32) return DS_ERR_ARG;
+  DS_TRY(raster_alloc_splats(rb, max_splats, cap));
+  rb.tile_size = tile_size;
+  rb.width = (int)pixels;  // batch: flat pixel count; per-instance sizes live in geom
+  rb.height = 1;
+  rb.ntx = tiles;
+  rb.nty = 1;
+  rb.tiles = tiles;
+  DS_TRY(alloc(&rb.ranges, (size_t)tiles));
+  DS_TRY(alloc(&rb.tile_order, (size_t)tiles));
+  DS_TRY(alloc(&rb.alphas, (size_t)pixels));
+  DS_TRY(alloc(&rb.last_ids, (size_t)pixels));
+  DS_TRY(alloc(&rb.loss_partials, (size_t)tiles));
+  DS_CUDA(cudaMemset(rb.ranges, 0, tiles * sizeof(int2)));
+  return DS_OK;
 }
 
 int raster_resize(RasterBuffers& rb, int width, int height) {
@@ -361,7 +394,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
     emit_kernel<<<(unsigned)(((int64_t)n * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
-        rb.tile_k0, rb.emit_splat, rb.seg_start);
+        rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom);
     DS_CUDA(cudaGetLastError());
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
     // 4) stable sort by tile id; last pass gathers the splat id of each pair

@@ -242,3 +242,26 @@ def orbit_cameras(count: int = 16, radius: float = 15.0, width: int = 1920, heig
                                     near, far)
         cams.append((pv, eye))
     return cams
+
+
+BATCH_SIZES = [(128, 128), (256, 256), (512, 512), (640, 480), (1024, 768)]
+
+
+def batch_problems(count: int = 64, seed: int = 0, nmin: int = 2000,
+                   nmax: int = 200_000) -> list:
+    """Uneven fitting instances built like the small plain fitter, each from its
+    own seed: image size drawn from BATCH_SIZES, splat count log-uniform in
+    [nmin, nmax], pinhole camera with fx = fy = width and a centred principal
+    point, procedural target with 200 blobs per 256x256 of area (at least 100)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    probs = []
+    for k in range(count):
+        W, H = BATCH_SIZES[int(rng.integers(0, len(BATCH_SIZES)))]
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        s = seed * 100_003 + k
+        blobs = max(100, int(200 * W * H / (256 * 256)))
+        f = float(W)
+        probs.append(FitProblem(W, H, random_splats(n, W, H, f, f, W / 2, H / 2, s + 1),
+                                make_target(W, H, blobs, s), pinhole_pv(W, H, f, f, W / 2, H / 2),
+                                np.zeros(3, np.float32), 0, PLAIN_SMALL_LRS))
+    return probs

@@ -272,6 +272,51 @@ int ds_fitter_pair_stats(ds_fitter *f, uint64_t *out, int n, ds_stream stream);
 int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
 int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
 
+/* ---- Batched fitting (no reference counterpart) ----
+ * Many independent ImageFitter-style instances of uneven image size and splat
+ * count stepped together: every stage is one launch over all instances, the
+ * step is captured once into a CUDA graph.  Splats of all instances share one
+ * parameter SoA (ds_batch_params, count = all splats; instance k owns columns
+ * [first, first + count) of ds_batch_instance_range); each instance has its
+ * own target, camera, image and loss.  tile_size 8, 16 or 32 and
+ * pixels_per_thread 1 or 2 select the composite kernels (16 is the
+ * reference's tile; other sizes change which splats a tile lists, not the
+ * compositing rule).  Default storage is BF16 (FP32 masters). */
+typedef struct ds_batch ds_batch;
+typedef struct ds_batch_instance {
+  int32_t width, height, count, reserved;
+} ds_batch_instance;
+typedef struct ds_batch_config {
+  int32_t instances;
+  int32_t sh_degree;
+  int64_t max_isects; /* all instances together; <= 0: 2^25 */
+  float lr_pos, lr_scale, lr_rot, lr_sh_dc, lr_sh_rest, lr_opacity;
+  float beta1, beta2, epsilon;
+  int32_t storage;
+  int32_t use_graph;
+  int32_t grad_mode;
+  int32_t schedule;
+  int32_t tile_size;         /* 8, 16 or 32 */
+  int32_t pixels_per_thread; /* 1 or 2 */
+} ds_batch_config;
+int ds_batch_default_config(ds_batch_config *cfg);
+int ds_batch_create(const ds_batch_config *cfg, const ds_batch_instance *instances,
+                    ds_batch **out);
+int ds_batch_params(ds_batch *b, ds_gaussian3d *out);
+int ds_batch_instance_range(ds_batch *b, int instance, int32_t *first_splat, int32_t *count);
+int ds_batch_params_updated(ds_batch *b);
+int ds_batch_set_target(ds_batch *b, int instance, const float *target, ds_stream stream);
+int ds_batch_set_camera(ds_batch *b, int instance, const float pv[16], const float cam_pos[3],
+                        ds_stream stream);
+int ds_batch_step(ds_batch *b, int n_steps, ds_stream stream);
+/* Per-instance losses of the most recent step (host array [instances]; synchronises). */
+int ds_batch_losses(ds_batch *b, float *losses, ds_stream stream);
+int ds_batch_output(ds_batch *b, int instance, float **image);
+/* out[0] = (tile, splat) pairs, out[1] = visible splats, out[2] = step count (synchronises). */
+int ds_batch_counters(ds_batch *b, uint64_t *out, int n);
+int ds_batch_status(ds_batch *b, uint32_t *flags);
+int ds_batch_destroy(ds_batch *b);
+
 /* ---- Forward-only renderer: SplatRenderer (src/pipelines/splat_renderer.h:17-60) ----
  * render() = GaussActiv -> PerspProject -> TileRasterize forward
  * (src/pipelines/splat_renderer.cpp:84-91) into an owned [H*W*3] image.

@@ -38,7 +38,8 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
     import subprocess
     from diffsplat_b200 import _lib as L
     structs = {"ds_gaussian3d": L.Gaussian3D, "ds_splat3d": L.Splat3D, "ds_splat2d": L.Splat2D,
-               "ds_adam_group": L.AdamGroup, "ds_fitter_config": L.FitterConfig}
+               "ds_adam_group": L.AdamGroup, "ds_fitter_config": L.FitterConfig,
+               "ds_batch_config": L.BatchConfig, "ds_batch_instance": L.BatchInstance}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "diffsplat_b200.h"',
              "int main(void) {"]
     expect = []
