@@ -152,6 +152,18 @@ _SIGS = {
     "ds_batch_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "ds_batch_status": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
     "ds_batch_destroy": (C.c_int, [_vp]),
+    "ds_gemm_bf16_tn": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int, _vp,
+                                  _vp, _vp]),
+    "ds_im2col_bf16": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                 _vp]),
+    "ds_col2im_bf16": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                 _vp, _vp]),
+    "ds_transpose_bf16": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
+    "ds_colsum_bf16": (C.c_int, [_vp, C.c_int64, C.c_int, _vp, C.c_int, _vp, _vp]),
+    "ds_adamw": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, C.c_float,
+                           C.c_float, C.c_float, C.c_int, _vp, _vp]),
+    "ds_cast_bf16": (C.c_int, [_vp, C.c_int64, _vp, _vp]),
     "ds_renderer_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int,
                                      C.POINTER(_vp)]),
     "ds_renderer_set_params": (C.c_int, [_vp, C.POINTER(Gaussian3D), _vp]),

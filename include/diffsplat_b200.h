@@ -317,6 +317,35 @@ int ds_batch_counters(ds_batch *b, uint64_t *out, int n);
 int ds_batch_status(ds_batch *b, uint32_t *flags);
 int ds_batch_destroy(ds_batch *b);
 
+/* ---- BF16 tensor-core kernels of the learned initializer (no reference counterpart) ----
+ * ds_gemm_bf16_tn: D[M,N] = A[M,K] . B[N,K]^T with A, B BF16 row-major (K
+ * inner, leading dimensions lda / ldb elements, 16-byte aligned rows) on
+ * tcgen05 tensor cores with FP32 accumulation.  epilogue 0: FP32 D (ldd);
+ * 1: Z = BF16(acc + bias), Y = BF16(gelu(acc + bias)) (ldy); 2: FP32 D = acc +
+ * bias.  splits > 1 (epilogue 0 only) splits K over CTAs into `workspace`
+ * [splits*M*ldd floats] and sums the splits in order.  *err becomes non-zero
+ * if a CTA's pipeline wait timed out (the result is then invalid). */
+int ds_gemm_bf16_tn(const void *A, int lda, const void *B, int ldb, int M, int N, int K,
+                    int epilogue, float *D, int ldd, void *Y, void *Z, int ldy, const float *bias,
+                    int splits, float *workspace, uint32_t *err, ds_stream stream);
+/* 3x3 convolution with padding 1 and stride 1 or 2 on NHWC BF16 tensors:
+ * im2col writes col[B*Ho*Wo][Kp] (k = (ky*3 + kx)*C + c, zero for k >= 9C);
+ * col2im sums dcol back onto dx[B][H][W][C] and multiplies by gelu'(z) when z
+ * is given. */
+int ds_im2col_bf16(const void *x, int B, int H, int W, int C, int stride, int Kp, void *col,
+                   ds_stream stream);
+int ds_col2im_bf16(const float *dcol, int B, int H, int W, int C, int stride, int Kp,
+                   const void *z, void *dx, ds_stream stream);
+int ds_transpose_bf16(const void *in, int rows, int cols, void *out, ds_stream stream);
+/* out[c] = sum_m a[m][c]; workspace holds max_parts * C floats. */
+int ds_colsum_bf16(const void *a, int64_t M, int C, float *workspace, int max_parts, float *out,
+                   ds_stream stream);
+/* AdamW on FP32 master weights (decoupled decay), optional BF16 copy out. */
+int ds_adamw(float *p, const float *g, float *m, float *v, int64_t n, float lr, float beta1,
+             float beta2, float eps, float weight_decay, int step, void *bf16_out,
+             ds_stream stream);
+int ds_cast_bf16(const float *in, int64_t n, void *out, ds_stream stream);
+
 /* ---- Forward-only renderer: SplatRenderer (src/pipelines/splat_renderer.h:17-60) ----
  * render() = GaussActiv -> PerspProject -> TileRasterize forward
  * (src/pipelines/splat_renderer.cpp:84-91) into an owned [H*W*3] image.
