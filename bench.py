@@ -430,6 +430,107 @@ def run_batch(args) -> dict:
             "n_isects": isects, "status": code, "clocks": clk.summary()}
 
 
+def gemm_tflops(M: int, N: int, K: int, reps: int = 10) -> float:
+    """Device TFLOP/s of the tcgen05 GEMM D = A . B^T (BF16 in, FP32 out)."""
+    import torch
+    from diffsplat_b200 import nn
+    A = torch.randn(M, K, device="cuda").to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda").to(torch.bfloat16)
+    D = torch.empty(M, N, device="cuda")
+    g = nn.Gemm()
+    for _ in range(3):
+        g(A, B, D=D)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        g(A, B, D=D)
+    b.record()
+    torch.cuda.synchronize()
+    g.check()
+    return 2.0 * M * N * K * reps / (a.elapsed_time(b) * 1e-3) / 1e12
+
+
+def run_init(args) -> dict:
+    """Learned initializer at 512^2: training pairs fitted by the batched BF16
+    fitter from the grid init, network training (AdamW, batch 32), and steps /
+    seconds to 28 dB on held-out targets for random, grid and learned inits,
+    plus learned init + batched BF16 fitting of all held-out targets at once."""
+    import torch
+    from diffsplat_b200 import api, initializer as I
+    from diffsplat_b200.scenes import PLAIN_SMALL_LRS
+    torch.cuda.set_device(0)
+    n_train, n_eval, fit_steps = 256, 16, 500
+    init = I.Initializer(512, seed=0)
+    t0 = time.perf_counter()
+    targets = I.make_targets_gpu(n_train + n_eval, 512, seed=11)
+    torch.cuda.synchronize()
+    t_targets = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fitted = I.fit_pairs(init, targets[:n_train], steps=fit_steps, batch=64)
+    t_pairs = time.perf_counter() - t0
+    # network forward at batch 32: algorithmic FLOPs 2 * Ho * Wo * Cout * 9 * Cin per layer
+    flops, h, cin = 0, 512, 3
+    for c, s in zip(I.CHANNELS, I.STRIDES):
+        h = (h - 1) // s + 1
+        flops += 2 * h * h * c * 9 * cin
+        cin = c
+    flops += 2 * h * h * 56 * 9 * cin
+    imgs = targets[:32].contiguous()
+    for _ in range(2):
+        init.forward(imgs)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(5):
+        init.forward(imgs)
+    b.record()
+    torch.cuda.synchronize()
+    fwd_ms = a.elapsed_time(b) / 5
+    t0 = time.perf_counter()
+    hist = I.train(init, targets[:n_train], fitted, steps=args.steps, batch=32, log_every=50)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    held = targets[n_train:]
+    ev = I.evaluate(init, held, goal=28.0, max_steps=2000)
+    # learned init + batched BF16 fitting of all held-out targets together
+    a.record()
+    out = init.forward(held.contiguous())
+    P = init.decode(out).cpu().numpy()
+    S = init.splats
+    bt = api.Batch([(512, 512, S)] * n_eval, lrs=PLAIN_SMALL_LRS, max_isects=n_eval * S * 16)
+    for k in range(n_eval):
+        bt.set_params(k, P[:, k * S:(k + 1) * S])
+        bt.set_target(k, held[k])
+        bt.set_camera(k, init.pv, init.cam)
+    steps = 0
+    while steps < 2000:
+        bt.step(10)
+        steps += 10
+        if min(I.psnr(x) for x in bt.losses()) >= 28.0:
+            break
+    b.record()
+    torch.cuda.synchronize()
+    batch_s = a.elapsed_time(b) / 1e3
+    final = [I.psnr(x) for x in bt.losses()]
+    bt.close()
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else {"bf16_tflops": 1590.0}
+    big = gemm_tflops(8192, 8192, 8192)
+    l5 = gemm_tflops(32 * 64 * 64, 256, 2304)
+    return {"train_pairs": n_train, "fit_steps": fit_steps, "eval_targets": n_eval,
+            "seconds": {"targets": t_targets, "pairs": t_pairs, "train": t_train},
+            "train_steps": args.steps, "train_history": hist,
+            "net_forward_ms_batch32": fwd_ms,
+            "net_forward_tflops": flops * 32 / (fwd_ms * 1e-3) / 1e12,
+            "gemm_tflops_8192cubed": big, "gemm_tflops_level5": l5,
+            "bf16_peak_tflops": peaks.get("bf16_tflops"),
+            "gemm_frac_8192cubed": big / peaks.get("bf16_tflops", 1590.0),
+            "eval": {k: v for k, v in ev.items() if k != "rows"},
+            "learned_batched_bf16_seconds_all": batch_s, "learned_batched_steps": steps,
+            "learned_batched_psnr_min": min(final),
+            "random_fp32_sequential_seconds_all": ev["random_seconds"] * n_eval,
+            "random_fp32_reached": ev["random_reached"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -440,13 +541,24 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="untimed: warmup + steps eager steps of the same workload with a "
                          "2^22-pair buffer (for ncu captures); prints no JSON line")
-    ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64"], default="fitter",
+    ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64", "init"],
+                    default="fitter",
                     help="fitter: the headline 1280x720 / 60000-splat training step; "
                          "viewer-sh3: 1M-splat SH-3 scene at 1920x1080, forward and fwd+bwd; "
-                         "batch64: 64 uneven instances in one batched step vs sequential")
+                         "batch64: 64 uneven instances in one batched step vs sequential; "
+                         "init: learned initializer training and seconds to 28 dB")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.workload == "init":
+        res = run_init(args)
+        print(json.dumps({
+            "metric": "wall-time to 28 dB PSNR, learned vs random init (512^2, 16384 splats)",
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": "5-level conv initializer 32-64-128-256-256, 64x64x4 splats, "
+                                   "512^2 procedural targets (500-3000 blobs)"},
+            "value": res["eval"]["learned_seconds"], **res}))
         return
     if args.workload == "batch64":
         res = run_batch(args)

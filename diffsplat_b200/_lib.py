@@ -164,6 +164,9 @@ _SIGS = {
     "ds_adamw": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, C.c_float,
                            C.c_float, C.c_float, C.c_int, _vp, _vp]),
     "ds_cast_bf16": (C.c_int, [_vp, C.c_int64, _vp, _vp]),
+    "ds_head_decode": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _fp, C.c_float, _vp, _vp]),
+    "ds_head_encode_grad": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_int, C.c_int, _fp,
+                                      _vp, _vp]),
     "ds_renderer_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int,
                                      C.POINTER(_vp)]),
     "ds_renderer_set_params": (C.c_int, [_vp, C.POINTER(Gaussian3D), _vp]),

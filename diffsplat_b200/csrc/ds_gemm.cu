@@ -429,11 +429,12 @@ __global__ void col2im_kernel(const float* __restrict__ dcol, int B, int H, int 
   }
 }
 
-// out[c][r] = in[r][c] through 32 x 32 shared-memory tiles.
+// out[c][r] = in[r][c] through 32 x 32 shared-memory tiles (blockIdx.x over
+// row tiles, which may exceed the 65535 limit of gridDim.y).
 __global__ void transpose_bf16_kernel(const __nv_bfloat16* __restrict__ in, int rows, int cols,
                                       __nv_bfloat16* __restrict__ out) {
   __shared__ __nv_bfloat16 t[32][33];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
     const int r = r0 + k, c = c0 + threadIdx.x;
     if (r < rows && c < cols) t[k][threadIdx.x] = in[(int64_t)r * cols + c];
@@ -490,6 +491,64 @@ __global__ void cast_bf16_kernel(const float* __restrict__ in, int64_t n,
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     out[i] = __float2bfloat16_rn(in[i]);
+}
+
+// Head of the learned initializer: per cell (i, j) of a G x G grid, 4 splats of
+// 14 channels {dx, dy, dz, log-scale xyz, quaternion wxyz, SH DC rgb, logit}.
+// Splat s = (i * G + j) * 4 + q of image b gets
+//   pos = base[s] + (dx, dy, dz) * step_xyz,  log-scale = base_ls + ls,
+//   quaternion = (1, 0, 0, 0) + q, DC and logit as predicted,
+// written to the field-major [14][B * S] parameter rows (S = 4 G^2).
+__global__ void head_decode_kernel(const float* __restrict__ out, int B, int G,
+                                   const float* __restrict__ base, float3 step, float base_ls,
+                                   float* __restrict__ params) {
+  const int S = 4 * G * G;
+  const int64_t total = (int64_t)B * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(t % S);
+    const int cell = s >> 2, q = s & 3;
+    const int64_t b = t / S;
+    const float* o = out + ((int64_t)b * G * G + cell) * 56 + q * 14;
+    const int64_t n = total;
+    params[0 * n + t] = base[3 * s + 0] + o[0] * step.x;
+    params[1 * n + t] = base[3 * s + 1] + o[1] * step.y;
+    params[2 * n + t] = base[3 * s + 2] + o[2] * step.z;
+    for (int k = 3; k < 6; ++k) params[k * n + t] = base_ls + o[k];
+    params[6 * n + t] = 1.f + o[6];
+    for (int k = 7; k < 14; ++k) params[k * n + t] = o[k];
+  }
+}
+
+// Gradient of the head output from parameter gradients (transpose of the
+// decode), combined with an L1 term: dparams = w_render * g_render +
+// w_l1 * sign(params - target), as BF16 [B * G * G][56].
+__global__ void head_encode_grad_kernel(const float* __restrict__ g_render,
+                                        const float* __restrict__ params,
+                                        const float* __restrict__ target, float w_render,
+                                        float w_l1, int B, int G, float3 step,
+                                        __nv_bfloat16* __restrict__ dout) {
+  const int S = 4 * G * G;
+  const int64_t total = (int64_t)B * S;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(t % S);
+    const int cell = s >> 2, q = s & 3;
+    const int64_t b = t / S;
+    __nv_bfloat16* o = dout + ((int64_t)b * G * G + cell) * 56 + q * 14;
+    for (int k = 0; k < 14; ++k) {
+      const int64_t i = (int64_t)k * total + t;
+      float g = g_render ? w_render * g_render[i] : 0.f;
+      if (target) {
+        const float d = params[i] - target[i];
+        g += w_l1 * (d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f));
+      }
+      if (k == 0) g *= step.x;
+      if (k == 1) g *= step.y;
+      if (k == 2) g *= step.z;
+      o[k] = __float2bfloat16_rn(g);
+    }
+  }
 }
 
 unsigned grid_for(int64_t n) {
@@ -572,7 +631,8 @@ int ds_col2im_bf16(const float* dcol, int B, int H, int W, int C, int stride, in
 
 int ds_transpose_bf16(const void* in, int rows, int cols, void* out, ds_stream stream) {
   if (!in || !out || rows <= 0 || cols <= 0) return DS_ERR_ARG;
-  dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+  if ((cols + 31) / 32 > 65535) return DS_ERR_ARG;
+  dim3 grid((rows + 31) / 32, (cols + 31) / 32);
   ds::transpose_bf16_kernel<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(
       (const __nv_bfloat16*)in, rows, cols, (__nv_bfloat16*)out);
   return ds::cuda_status(cudaGetLastError());
@@ -598,6 +658,26 @@ int ds_adamw(float* p, const float* g, float* m, float* v, int64_t n, float lr, 
   const float bc2 = 1.f / (1.f - powf(beta2, (float)step));
   ds::adamw_kernel<<<ds::grid_for(n), 256, 0, (cudaStream_t)stream>>>(
       p, g, m, v, n, lr, beta1, beta2, eps, weight_decay, bc1, bc2, (__nv_bfloat16*)bf16_out);
+  return ds::cuda_status(cudaGetLastError());
+}
+
+int ds_head_decode(const float* out, int B, int G, const float* base, const float step[3],
+                   float base_log_scale, float* params, ds_stream stream) {
+  if (!out || !base || !step || !params || B <= 0 || G <= 0) return DS_ERR_ARG;
+  const int64_t n = (int64_t)B * 4 * G * G;
+  ds::head_decode_kernel<<<ds::grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+      out, B, G, base, make_float3(step[0], step[1], step[2]), base_log_scale, params);
+  return ds::cuda_status(cudaGetLastError());
+}
+
+int ds_head_encode_grad(const float* g_render, const float* params, const float* target,
+                        float w_render, float w_l1, int B, int G, const float step[3], void* dout,
+                        ds_stream stream) {
+  if (!params || !step || !dout || B <= 0 || G <= 0) return DS_ERR_ARG;
+  const int64_t n = (int64_t)B * 4 * G * G;
+  ds::head_encode_grad_kernel<<<ds::grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+      g_render, params, target, w_render, w_l1, B, G, make_float3(step[0], step[1], step[2]),
+      (__nv_bfloat16*)dout);
   return ds::cuda_status(cudaGetLastError());
 }
 

@@ -345,6 +345,17 @@ int ds_adamw(float *p, const float *g, float *m, float *v, int64_t n, float lr, 
              float beta2, float eps, float weight_decay, int step, void *bf16_out,
              ds_stream stream);
 int ds_cast_bf16(const float *in, int64_t n, void *out, ds_stream stream);
+/* Initializer head on a G x G grid, 4 splats per cell, 14 channels per splat
+ * {dx, dy, dz, log-scale xyz, quaternion wxyz, SH DC rgb, logit}: decode the
+ * FP32 head output [B*G*G][56] into field-major parameter rows [14][B*4*G*G]
+ * (pos = base + d * step, log-scale = base_log_scale + ls, quaternion =
+ * (1,0,0,0) + q), and map parameter gradients back (w_render * g_render +
+ * w_l1 * sign(params - target); either term optional) as BF16 [B*G*G][56]. */
+int ds_head_decode(const float *out, int B, int G, const float *base, const float step[3],
+                   float base_log_scale, float *params, ds_stream stream);
+int ds_head_encode_grad(const float *g_render, const float *params, const float *target,
+                        float w_render, float w_l1, int B, int G, const float step[3], void *dout,
+                        ds_stream stream);
 
 /* ---- Forward-only renderer: SplatRenderer (src/pipelines/splat_renderer.h:17-60) ----
  * render() = GaussActiv -> PerspProject -> TileRasterize forward
