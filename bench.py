@@ -541,6 +541,8 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="untimed: warmup + steps eager steps of the same workload with a "
                          "2^22-pair buffer (for ncu captures); prints no JSON line")
+    ap.add_argument("--gemm", default=None, metavar="M,N,K",
+                    help="time one BF16 tensor-core GEMM shape and print its TFLOP/s")
     ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64", "init"],
                     default="fitter",
                     help="fitter: the headline 1280x720 / 60000-splat training step; "
@@ -550,6 +552,14 @@ def main():
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.gemm:
+        import torch
+        torch.cuda.set_device(0)
+        M, N, K = (int(x) for x in args.gemm.split(","))
+        tf = gemm_tflops(M, N, K, reps=max(1, args.steps))
+        print(json.dumps({"metric": "tcgen05 BF16 GEMM TFLOP/s", "M": M, "N": N, "K": K,
+                          "value": tf, "unit": "TFLOP/s"}))
         return
     if args.workload == "init":
         res = run_init(args)

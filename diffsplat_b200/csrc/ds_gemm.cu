@@ -570,7 +570,16 @@ int ds_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb, int M, int N
   if (epilogue != ds::kEpiBiasGeluBf16 && (!D || ldd < N)) return DS_ERR_ARG;
   if (splits < 1) splits = 1;
   if (splits > 1 && (epilogue != ds::kEpiF32 || !workspace)) return DS_ERR_ARG;
-  const int bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  // Widest tile that covers N, narrowed while the grid leaves SMs idle.
+  int bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  const int64_t mt = (M + ds::kBM - 1) / ds::kBM;
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  while (bn > 64 && mt * ((N + bn - 1) / bn) * splits < sms) bn /= 2;
   CUtensorMap ma, mb;
   DS_TRY(ds::make_map(&ma, A, M, K, lda, ds::kBM));
   DS_TRY(ds::make_map(&mb, B, N, K, ldb, bn));
