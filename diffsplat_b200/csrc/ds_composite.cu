@@ -110,12 +110,44 @@ __device__ __forceinline__ bool misses(const float4& a, const float4& box) {
   return a.x + a.z < box.x || a.x - a.z > box.y || a.y + a.w < box.z || a.y - a.w > box.w;
 }
 
-// Bit w set: the splat's acceptance box overlaps warp w's pixel block.
+// Whether any point of a warp's pixel box can reach the splat's sigma cut:
+// the minimum over the box of a lower bound of the conic's quadratic form
+// (diagonal shrunk by 1e-5 relative, as for the acceptance box) is at the
+// centre when the box holds it, else at the clamped stationary point of one
+// of the four edges.  The 0.01 of slack in the cut covers the rounding, so a
+// pixel that can pass the per-pixel tests is never skipped.
+__device__ __forceinline__ bool ellipse_hits(const float4& a, const float4& b, float cut,
+                                             const float4& box) {
+  if (misses(a, box)) return false;
+  if (!(a.z <= 3.0e38f && a.w <= 3.0e38f)) return true;  // unbounded region
+  const float x0 = box.x - a.x, x1 = box.y - a.x, y0 = box.z - a.y, y1 = box.w - a.y;
+  if (x0 <= 0.f && x1 >= 0.f && y0 <= 0.f && y1 >= 0.f) return true;
+  const float k = 1e-5f;
+  const float qa = b.x - k * (fabsf(b.x) + fabsf(b.y));
+  const float qc = b.z - k * (fabsf(b.z) + fabsf(b.y));
+  const float qb = b.y;
+  if (!(qa > 0.f && qc > 0.f)) return true;
+  const float ia = 1.f / qa, ic = 1.f / qc;
+  float m = 3.0e38f;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const float X = e ? x1 : x0;
+    const float y = fminf(fmaxf(-qb * X * ic, y0), y1);
+    m = fminf(m, qa * X * X + 2.f * qb * X * y + qc * y * y);
+    const float Y = e ? y1 : y0;
+    const float x = fminf(fmaxf(-qb * Y * ia, x0), x1);
+    m = fminf(m, qa * x * x + 2.f * qb * x * Y + qc * Y * Y);
+  }
+  return 0.5f * m <= cut;
+}
+
+// Bit w set: the splat can reach warp w's pixel block.
 template <int NW>
-__device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4* box) {
+__device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4& b, float cut,
+                                              const float4* box) {
   uint32_t mk = 0;
 #pragma unroll
-  for (int w = 0; w < NW; ++w) mk |= misses(a, box[w]) ? 0u : (1u << w);
+  for (int w = 0; w < NW; ++w) mk |= ellipse_hits(a, b, cut, box[w]) ? (1u << w) : 0u;
   return mk;
 }
 
@@ -167,11 +199,11 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
       uint32_t mk = 0u;
       if (idx < end) {
         const uint32_t g = sorted_splat[idx];
-        const float4 a = ra[g];
+        const float4 a = ra[g], bb = rb[g], cc = rc[g];
         sA[l] = a;
-        sB[l] = rb[g];
-        sC[l] = rc[g];
-        mk = warp_hits<NW>(a, sBox);
+        sB[l] = bb;
+        sC[l] = cc;
+        mk = warp_hits<NW>(a, bb, cc.w, sBox);
       }
       sMask[l] = mk;
     }
@@ -346,12 +378,12 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
       uint32_t mk = 0u;
       if (li >= start) {
         const uint32_t g = sorted_splat[li];
-        const float4 a = ra[g];
+        const float4 a = ra[g], bb = rb[g], cc = rc[g];
         sA[l] = a;
-        sB[l] = rb[g];
-        sC[l] = rc[g];
+        sB[l] = bb;
+        sC[l] = cc;
         sI[l] = ridet[g];
-        mk = warp_hits<NW>(a, sBox);
+        mk = warp_hits<NW>(a, bb, cc.w, sBox);
       }
       sMask[l] = mk;
     }
