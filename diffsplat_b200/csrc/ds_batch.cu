@@ -280,6 +280,7 @@ int ds_batch_create(const ds_batch_config* cfg, const ds_batch_instance* inst, d
   b->rb.grad_mode = cfg->grad_mode;
   b->rb.schedule = cfg->schedule;
   b->rb.ppt = cfg->pixels_per_thread;
+  b->rb.ppt_bwd = cfg->pixels_per_thread;
   b->rb.inst_of_splat = b->inst_of_splat;
   b->rb.tile_inst = b->tile_inst;
   b->rb.geom = b->geom_dev;

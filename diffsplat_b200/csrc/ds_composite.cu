@@ -40,8 +40,8 @@ struct Lay {
   static constexpr int BH = 32 * PPT / BW;      // warp block height
   static constexpr int kLaneRows = 32 / BW;     // rows between a thread's pixels
   static constexpr int kWarpsX = TS / BW;
-  // backward batch: the per-warp partials (kWarps x kBwdBatch x 36 B) stay at 18 KB
-  static constexpr int kBwdBatch = 512 / kWarps < 256 ? 512 / kWarps : 256;
+  // backward batch: the per-warp partials (kWarps x kBwdBatch x 36 B) stay within 36 KB
+  static constexpr int kBwdBatch = 1024 / kWarps < 128 ? 1024 / kWarps : 128;
   static_assert(kThreads % 32 == 0 && BW <= TS && kWarps <= 32, "unsupported tile layout");
 };
 
@@ -542,15 +542,16 @@ struct BwdOp {
 // Single instance: 16x16 tiles, PPT 1, 2 or 4.  Batch: tiles of 8, 16 or 32
 // pixels with PPT 1 or 2.
 template <class F>
-int dispatch(const RasterBuffers& rb, const F& f) {
+int dispatch(const RasterBuffers& rb, const F& f, bool backward = false) {
+  const int ppt = backward ? rb.ppt_bwd : rb.ppt;
   if (!rb.geom) {
-    switch (rb.ppt) {
+    switch (ppt) {
       case 4: f.template run<4, 16, false>(); return DS_OK;
       case 2: f.template run<2, 16, false>(); return DS_OK;
       default: f.template run<1, 16, false>(); return DS_OK;
     }
   }
-  const bool two = rb.ppt == 2;
+  const bool two = ppt == 2;
   switch (rb.tile_size) {
     case 8:
       if (two) f.template run<2, 8, true>();
@@ -580,6 +581,15 @@ int composite_default_ppt() {
   return 1;
 }
 
+int composite_default_ppt_bwd() {
+  const char* e = getenv("DS_COMPOSITE_PPT_BWD");
+  if (e) {
+    int v = atoi(e);
+    if (v == 1 || v == 2 || v == 4) return v;
+  }
+  return composite_default_ppt();
+}
+
 bool composite_longest_first() {
   static const bool on = [] {
     const char* e = getenv("DS_TILE_SCHEDULE");
@@ -602,7 +612,7 @@ int raster_composite_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
 
 int raster_composite_backward(RasterBuffers& rb, const float* image, const float* grad_rgb,
                               const float* target, cudaStream_t s) {
-  dispatch(rb, BwdOp{rb, image, grad_rgb, target, s});
+  dispatch(rb, BwdOp{rb, image, grad_rgb, target, s}, true);
   return cuda_status(cudaGetLastError());
 }
 

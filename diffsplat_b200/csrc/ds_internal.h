@@ -97,7 +97,8 @@ struct RasterBuffers {
   int max_splats = 0;
   int64_t cap = 0;  // intersection capacity
   int grad_mode = DS_GRAD_REFERENCE;
-  int ppt = 2;  // pixels per thread of the composite kernels (1, 2 or 4)
+  int ppt = 2;      // pixels per thread of the composite forward (1, 2 or 4)
+  int ppt_bwd = 2;  // pixels per thread of the composite backward
   int schedule = DS_SCHEDULE_LONGEST_FIRST;  // composite tile order
   int tile_size = 16;  // pixels per tile edge: 16 (reference); batches may use 8 or 32
 
@@ -157,6 +158,7 @@ int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64
 // Pixels per thread of the composite kernels; DS_COMPOSITE_PPT=1|2|4 overrides
 // the default (a tuning knob: results are identical for every value).
 int composite_default_ppt();
+int composite_default_ppt_bwd();
 // Composite CTA schedule: longest tile lists first (default) or raster order
 // (DS_TILE_SCHEDULE=raster).
 bool composite_longest_first();

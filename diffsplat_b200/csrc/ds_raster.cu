@@ -252,6 +252,7 @@ static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   rb.max_splats = max_splats;
   rb.cap = cap;
   rb.ppt = composite_default_ppt();
+  rb.ppt_bwd = composite_default_ppt_bwd();
   rb.schedule = composite_longest_first() ? DS_SCHEDULE_LONGEST_FIRST : DS_SCHEDULE_RASTER;
   const size_t n = (size_t)max_splats;
   DS_TRY(alloc(&rb.rec_a, n));
