@@ -167,6 +167,12 @@ _SIGS = {
     "ds_head_decode": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _fp, C.c_float, _vp, _vp]),
     "ds_head_encode_grad": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_int, C.c_int, _fp,
                                       _vp, _vp]),
+    "ds_image_probe": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ds_image_read_rgb8": (C.c_int, [C.c_char_p, _vp, C.c_int64, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
+    "ds_image_fit": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                               C.POINTER(C.c_int), C.POINTER(C.c_int), _vp]),
+    "ds_image_write_png": (C.c_int, [C.c_char_p, _vp, C.c_int, C.c_int]),
     "ds_renderer_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int,
                                      C.POINTER(_vp)]),
     "ds_renderer_set_params": (C.c_int, [_vp, C.POINTER(Gaussian3D), _vp]),

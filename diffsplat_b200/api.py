@@ -535,3 +535,38 @@ class Batch:
         flags = C.c_uint32()
         code = L.lib().ds_batch_status(self.h, C.byref(flags))
         return code, int(flags.value)
+
+
+# ---- image targets -------------------------------------------------------------
+
+def read_image(path) -> np.ndarray:
+    """PNG / PPM / PGM -> [H, W, 3] uint8 (ImageLoader's decode step)."""
+    p = str(path).encode()
+    w, h = C.c_int(), C.c_int()
+    L.call("ds_image_probe", p, C.byref(w), C.byref(h))
+    out = np.zeros((h.value, w.value, 3), np.uint8)
+    L.call("ds_image_read_rgb8", p, out.ctypes.data, out.size, C.byref(w), C.byref(h))
+    return out
+
+
+def fit_image(rgb8: np.ndarray, width: int, height: int, padding: int = 0, stream=None):
+    """Aspect fit + pad of an RGB8 image onto a [height, width, 3] float canvas on
+    the GPU (ImageLoader::load's resize and placement).  Returns (canvas, (fit_w, fit_h))."""
+    src = torch.as_tensor(np.ascontiguousarray(rgb8, np.uint8), device="cuda")
+    out = torch.empty(height, width, 3, dtype=torch.float32, device="cuda")
+    fw, fh = C.c_int(), C.c_int()
+    L.call("ds_image_fit", src.data_ptr(), rgb8.shape[1], rgb8.shape[0], width, height, padding,
+           out.data_ptr(), C.byref(fw), C.byref(fh), _stream(stream))
+    torch.cuda.current_stream().synchronize()
+    return out, (fw.value, fh.value)
+
+
+def load_image(path, width: int, height: int, padding: int = 0):
+    return fit_image(read_image(path), width, height, padding)
+
+
+def write_png(path, rgb) -> None:
+    """ImageSaver::saveAsPNG of an RGB float image in [0, 1] ([H, W, 3])."""
+    a = np.ascontiguousarray(rgb.detach().cpu().numpy() if torch.is_tensor(rgb) else rgb,
+                             np.float32)
+    L.call("ds_image_write_png", str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0])

@@ -357,6 +357,20 @@ int ds_head_encode_grad(const float *g_render, const float *params, const float 
                         float w_render, float w_l1, int B, int G, const float step[3], void *dout,
                         ds_stream stream);
 
+/* ---- Image targets: ImageLoader / ImageSaver (src/io/image_io.h:17-47) ----
+ * Decoding on the host: PNG (8-bit, non-interlaced; grey, grey+alpha, RGB,
+ * RGBA, palette) and binary PPM / PGM, to 8-bit RGB (JPEG is not supported).
+ * ds_image_fit: aspect-preserving fit of a device RGB8 image into a device
+ * float canvas [H*W*3] with `padding` pixels of margin, centred, black
+ * outside, values / 255 (area filter when shrinking, bilinear when
+ * enlarging).  ds_image_write_png: host RGB float in [0, 1] -> 8-bit PNG. */
+int ds_image_probe(const char *path, int *width, int *height);
+int ds_image_read_rgb8(const char *path, uint8_t *rgb, int64_t capacity, int *width,
+                       int *height);
+int ds_image_fit(const uint8_t *src_rgb, int src_w, int src_h, int canvas_w, int canvas_h,
+                 int padding, float *dst_rgb, int *fit_w, int *fit_h, ds_stream stream);
+int ds_image_write_png(const char *path, const float *rgb, int width, int height);
+
 /* ---- Forward-only renderer: SplatRenderer (src/pipelines/splat_renderer.h:17-60) ----
  * render() = GaussActiv -> PerspProject -> TileRasterize forward
  * (src/pipelines/splat_renderer.cpp:84-91) into an owned [H*W*3] image.
