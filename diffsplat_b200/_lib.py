@@ -70,7 +70,7 @@ class FitterConfig(C.Structure):
                 ("lr_sh_dc", C.c_float), ("lr_sh_rest", C.c_float), ("lr_opacity", C.c_float),
                 ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float),
                 ("storage", C.c_int32), ("use_graph", C.c_int32), ("grad_mode", C.c_int32),
-                ("schedule", C.c_int32)]
+                ("schedule", C.c_int32), ("capacity", C.c_int32)]
 
 
 GAUSSIAN3D_FIELDS = ("pos_x", "pos_y", "pos_z", "scale_x", "scale_y", "scale_z",
@@ -78,6 +78,11 @@ GAUSSIAN3D_FIELDS = ("pos_x", "pos_y", "pos_z", "scale_x", "scale_y", "scale_z",
                      "logit_opacity")
 SPLAT3D_FIELDS = tuple(n for n, _ in Splat3D._fields_[:-1])
 SPLAT2D_FIELDS = tuple(n for n, _ in Splat2D._fields_[:-1])
+
+class DensifyParams(C.Structure):
+    _fields_ = [("grad_threshold", C.c_float), ("scale_threshold", C.c_float),
+                ("min_opacity", C.c_float), ("seed", C.c_uint32)]
+
 
 class BatchInstance(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("count", C.c_int32),
@@ -137,6 +142,8 @@ _SIGS = {
     "ds_fitter_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "ds_fitter_pair_stats": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int, _vp]),
     "ds_fitter_params_updated": (C.c_int, [_vp]),
+    "ds_fitter_densify": (C.c_int, [_vp, C.POINTER(DensifyParams), C.POINTER(C.c_int32), _vp]),
+    "ds_fitter_density_stats": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
     "ds_batch_default_config": (C.c_int, [C.POINTER(BatchConfig)]),
     "ds_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(BatchInstance),
                                   C.POINTER(_vp)]),

@@ -233,13 +233,22 @@ def adam_step(groups, step: int, beta1=0.9, beta2=0.999, eps=1e-8, stream=None) 
 
 
 # ---- fused fitter ----------------------------------------------------------------------
+class _CountView:
+    """uint32 device vector view (cuda array interface)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<u4", "data": (ptr, False),
+                                          "version": 3, "strides": None}
+
+
 class Fitter:
     """Owns a ds_fitter (the graph-captured ImageFitter::step)."""
 
     def __init__(self, width: int, height: int, count: int, sh_degree: int = 0, lrs=None,
                  max_isects: int = 0, use_graph: bool = True, keep_grads: bool = False,
                  storage: int = L.DS_STORAGE_FP32, betas=(0.9, 0.999), eps: float = 1e-8,
-                 grad_mode: int = L.DS_GRAD_REFERENCE, schedule: int | None = None):
+                 grad_mode: int = L.DS_GRAD_REFERENCE, schedule: int | None = None,
+                 capacity: int = 0):
         cfg = L.FitterConfig()
         L.call("ds_fitter_default_config", C.byref(cfg))
         cfg.width, cfg.height, cfg.count, cfg.sh_degree = width, height, count, sh_degree
@@ -254,6 +263,7 @@ class Fitter:
         cfg.grad_mode = grad_mode
         if schedule is not None:
             cfg.schedule = schedule
+        cfg.capacity = capacity
         h = C.c_void_p()
         L.call("ds_fitter_create_with_grads" if keep_grads else "ds_fitter_create", C.byref(cfg),
                C.byref(h))
@@ -279,6 +289,27 @@ class Fitter:
     def set_params(self, params) -> None:
         self.params.copy_(torch.as_tensor(params, device="cuda"))
         L.call("ds_fitter_params_updated", self.h)
+
+    def densify(self, grad_threshold: float, scale_threshold: float, min_opacity: float = 0.005,
+                seed: int = 0, stream=None) -> int:
+        """Prune / clone / split from the accumulated gradient statistics (needs
+        capacity > count at creation); returns the new splat count."""
+        p = L.DensifyParams(grad_threshold, scale_threshold, min_opacity, seed)
+        n = C.c_int32()
+        L.call("ds_fitter_densify", self.h, C.byref(p), C.byref(n), _stream(stream))
+        g = L.Gaussian3D()
+        L.call("ds_fitter_params", self.h, C.byref(g))
+        self.params = g3_tensor_from_view(g)
+        self.count = n.value
+        return n.value
+
+    def density_stats(self):
+        """(gradient-norm sums, visible steps) per splat as CUDA tensors."""
+        a, c = C.c_void_p(), C.c_void_p()
+        L.call("ds_fitter_density_stats", self.h, C.byref(a), C.byref(c))
+        g = _wrap_device(a.value, (self.count,))
+        cnt = torch.as_tensor(_CountView(c.value, self.count), device="cuda")
+        return g, cnt
 
     def set_target(self, target: torch.Tensor, stream=None) -> None:
         target = target.contiguous()

@@ -43,6 +43,9 @@ struct ds_fitter {
   __nv_bfloat16* render_mem = nullptr;
   ds::Soa<__nv_bfloat16> R16{}, M16{}, V16{};
   bool render_dirty = true;
+  int capacity = 0;               // splats the raster buffers hold (densification room)
+  float* grad_accum = nullptr;    // densification statistics [capacity]
+  uint32_t* grad_count = nullptr;
   float* target = nullptr;
   float* image = nullptr;
   ds::RasterBuffers rb;
@@ -92,13 +95,14 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   AdamHyper h{f->cfg.beta1, f->cfg.beta2, f->cfg.epsilon};
   const int keep = f->g_mem ? 1 : 0, exact = f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0;
   if (bf16)
-    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(f->P, f->R16, f->M16, f->V16, f->G, keep,
-                                                         exact, f->cfg.sh_degree, f->cam_dev,
-                                                         rb.g2, f->bc_cur, rb.scalars, lr, h);
+    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
+        f->P, f->R16, f->M16, f->V16, f->G, keep, exact, f->cfg.sh_degree, f->cam_dev, rb.g2,
+        f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum, f->grad_count);
   else
     fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
         f->P, soa_of(f->P), soa_of(f->M), soa_of(f->V), f->G, keep, exact, f->cfg.sh_degree,
-        f->cam_dev, rb.g2, f->bc_cur, rb.scalars, lr, h);
+        f->cam_dev, rb.g2, f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum,
+        f->grad_count);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[7], s));
   return DS_OK;
@@ -154,6 +158,8 @@ int ds_fitter_destroy(ds_fitter* f) {
   cudaFree(f->v_mem);
   cudaFree(f->g_mem);
   cudaFree(f->render_mem);
+  cudaFree(f->grad_accum);
+  cudaFree(f->grad_count);
   cudaFree(f->target);
   cudaFree(f->image);
   cudaFree(f->cam_dev);
@@ -215,7 +221,15 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
   if ((st = ds::cuda_status(cudaMalloc(&f->target, px * 3 * 4)))) return fail(st);
   if ((st = ds::cuda_status(cudaMalloc(&f->image, px * 3 * 4)))) return fail(st);
   cudaMemset(f->image, 0, px * 3 * 4);
-  if ((st = ds::raster_alloc(f->rb, cfg->width, cfg->height, n, cfg->max_isects))) return fail(st);
+  f->capacity = std::max(n, cfg->capacity);
+  if ((st = ds::raster_alloc(f->rb, cfg->width, cfg->height, f->capacity, cfg->max_isects)))
+    return fail(st);
+  if (f->capacity > n) {
+    if ((st = ds::cuda_status(cudaMalloc(&f->grad_accum, (size_t)f->capacity * 4)))) return fail(st);
+    if ((st = ds::cuda_status(cudaMalloc(&f->grad_count, (size_t)f->capacity * 4)))) return fail(st);
+    cudaMemset(f->grad_accum, 0, (size_t)f->capacity * 4);
+    cudaMemset(f->grad_count, 0, (size_t)f->capacity * 4);
+  }
   f->rb.grad_mode = cfg->grad_mode;
   f->rb.schedule = cfg->schedule;
   if ((st = ds::cuda_status(cudaMalloc(&f->cam_dev, sizeof(ds::Camera))))) return fail(st);
@@ -392,6 +406,207 @@ int ds_fitter_moments(ds_fitter* f, ds_gaussian3d* m, ds_gaussian3d* v) {
   if (f->cfg.storage != DS_STORAGE_FP32) return DS_ERR_STATE;
   *m = f->M;
   *v = f->V;
+  return DS_OK;
+}
+
+}  // extern "C"
+
+// ---- adaptive density control ------------------------------------------------
+namespace ds {
+namespace {
+
+// Per splat: 0 pruned, 1 kept, 2 kept + clone, 3 split into two children.
+__global__ void densify_decide_kernel(ds_gaussian3d P, const float* __restrict__ gsum,
+                                      const uint32_t* __restrict__ gcnt, ds_densify_params dp,
+                                      uint8_t* __restrict__ mode, uint32_t* __restrict__ emit) {
+  const int n = P.count;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float op = 1.f / (1.f + expf(-P.logit_opacity[i]));
+  uint8_t m = 1;
+  if (op < dp.min_opacity) {
+    m = 0;
+  } else if (gcnt[i] > 0u && gsum[i] / (float)gcnt[i] >= dp.grad_threshold) {
+    const float smax = expf(fmaxf(P.scale_x[i], fmaxf(P.scale_y[i], P.scale_z[i])));
+    m = smax <= dp.scale_threshold ? 2 : 3;
+  }
+  mode[i] = m;
+  emit[i] = m == 0 ? 0u : (m == 1 ? 1u : 2u);
+}
+
+// Standard normal deviate from two hash draws (Box-Muller).
+__device__ __forceinline__ float gauss(uint32_t key) {
+  const float u1 = ((mix32(key) >> 8) + 1u) * (1.f / 16777217.f);
+  const float u2 = (mix32(key ^ 0x9e3779b9u) >> 8) * (1.f / 16777216.f);
+  return sqrtf(-2.f * logf(u1)) * cosf(6.28318530718f * u2);
+}
+
+__global__ void densify_scatter_kernel(ds_gaussian3d P, ds_gaussian3d M, ds_gaussian3d V,
+                                       const uint8_t* __restrict__ mode,
+                                       const unsigned long long* __restrict__ offs,
+                                       ds_gaussian3d Q, ds_gaussian3d MQ, ds_gaussian3d VQ,
+                                       uint32_t seed) {
+  const int n = P.count, nq = Q.count, nb = P.sh_num_bands;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || mode[i] == 0) return;
+  const int dst = (int)offs[i];
+  auto field = [](const ds_gaussian3d& g, int k) -> float* {
+    switch (k) {
+      case 0: return g.pos_x;
+      case 1: return g.pos_y;
+      case 2: return g.pos_z;
+      case 3: return g.scale_x;
+      case 4: return g.scale_y;
+      case 5: return g.scale_z;
+      case 6: return g.rot_w;
+      case 7: return g.rot_x;
+      case 8: return g.rot_y;
+      case 9: return g.rot_z;
+      case 10: return g.sh_dc_r;
+      case 11: return g.sh_dc_g;
+      case 12: return g.sh_dc_b;
+      default: return g.logit_opacity;
+    }
+  };
+  const uint8_t m = mode[i];
+  const int copies = m == 1 ? 1 : 2;
+  for (int c = 0; c < copies; ++c) {
+    const int j = dst + c;
+    const bool fresh = m == 3 || c == 1;  // new splats start from zero moments
+    for (int k = 0; k < 14; ++k) {
+      field(Q, k)[j] = field(P, k)[i];
+      field(MQ, k)[j] = fresh ? 0.f : field(M, k)[i];
+      field(VQ, k)[j] = fresh ? 0.f : field(V, k)[i];
+    }
+    for (int b = 0; b < nb; ++b) {
+      const float* ps[3] = {P.sh_rest_r, P.sh_rest_g, P.sh_rest_b};
+      float* qs[3] = {Q.sh_rest_r, Q.sh_rest_g, Q.sh_rest_b};
+      const float* ms[3] = {M.sh_rest_r, M.sh_rest_g, M.sh_rest_b};
+      float* mq[3] = {MQ.sh_rest_r, MQ.sh_rest_g, MQ.sh_rest_b};
+      const float* vs[3] = {V.sh_rest_r, V.sh_rest_g, V.sh_rest_b};
+      float* vq[3] = {VQ.sh_rest_r, VQ.sh_rest_g, VQ.sh_rest_b};
+      for (int ch = 0; ch < 3; ++ch) {
+        qs[ch][(int64_t)b * nq + j] = ps[ch][(int64_t)b * n + i];
+        mq[ch][(int64_t)b * nq + j] = fresh ? 0.f : ms[ch][(int64_t)b * n + i];
+        vq[ch][(int64_t)b * nq + j] = fresh ? 0.f : vs[ch][(int64_t)b * n + i];
+      }
+    }
+    if (m == 3) {
+      // child of a split: position drawn from the parent's Gaussian, scales / 1.6
+      UnitQuat q = unit_quat(P.rot_w[i], P.rot_x[i], P.rot_y[i], P.rot_z[i]);
+      Rot3 R = rot_from_quat(q.w, q.x, q.y, q.z);
+      const uint32_t key = mix32(seed) ^ mix32((uint32_t)i * 2u + (uint32_t)c);
+      const float sx = expf(P.scale_x[i]) * gauss(key * 3u + 0u);
+      const float sy = expf(P.scale_y[i]) * gauss(key * 3u + 1u);
+      const float sz = expf(P.scale_z[i]) * gauss(key * 3u + 2u);
+      Q.pos_x[j] = P.pos_x[i] + R.r00 * sx + R.r01 * sy + R.r02 * sz;
+      Q.pos_y[j] = P.pos_y[i] + R.r10 * sx + R.r11 * sy + R.r12 * sz;
+      Q.pos_z[j] = P.pos_z[i] + R.r20 * sx + R.r21 * sy + R.r22 * sz;
+      const float shrink = logf(1.6f);
+      Q.scale_x[j] = P.scale_x[i] - shrink;
+      Q.scale_y[j] = P.scale_y[i] - shrink;
+      Q.scale_z[j] = P.scale_z[i] - shrink;
+    }
+  }
+}
+
+}  // namespace
+}  // namespace ds
+
+extern "C" {
+
+int ds_fitter_densify(ds_fitter* f, const ds_densify_params* p, int32_t* new_count,
+                      ds_stream stream) {
+  if (!f || !p || !new_count) return DS_ERR_ARG;
+  if (!f->grad_accum || f->cfg.storage != DS_STORAGE_FP32 || f->g_mem) return DS_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = f->cfg.count;
+  uint8_t* mode = nullptr;
+  uint32_t *emit = nullptr, *iota = nullptr, *total32 = nullptr, *status = nullptr;
+  unsigned long long *offs = nullptr, *total = nullptr;
+  float *np = nullptr, *nm = nullptr, *nv = nullptr;
+  int st = DS_OK;
+  auto cleanup = [&]() {
+    for (void* q : {(void*)mode, (void*)emit, (void*)iota, (void*)total32, (void*)status,
+                    (void*)offs, (void*)total, (void*)np, (void*)nm, (void*)nv})
+      cudaFree(q);
+  };
+  auto fail = [&](int code) {
+    cleanup();
+    return code;
+  };
+  if ((st = ds::cuda_status(cudaMalloc(&mode, n))) ||
+      (st = ds::cuda_status(cudaMalloc(&emit, (size_t)n * 4))) ||
+      (st = ds::cuda_status(cudaMalloc(&iota, (size_t)n * 4))) ||
+      (st = ds::cuda_status(cudaMalloc(&offs, (size_t)n * 8))) ||
+      (st = ds::cuda_status(cudaMalloc(&total, 8))) ||
+      (st = ds::cuda_status(cudaMalloc(&total32, 4))) ||
+      (st = ds::cuda_status(cudaMalloc(&status, 4))))
+    return fail(st);
+  std::vector<uint32_t> h_iota(n);
+  for (int k = 0; k < n; ++k) h_iota[k] = (uint32_t)k;
+  if ((st = ds::cuda_status(cudaMemcpyAsync(iota, h_iota.data(), (size_t)n * 4,
+                                            cudaMemcpyHostToDevice, s))))
+    return fail(st);
+  const int blocks = (n + ds::kThreads - 1) / ds::kThreads;
+  ds::densify_decide_kernel<<<blocks, ds::kThreads, 0, s>>>(f->P, f->grad_accum, f->grad_count,
+                                                            *p, mode, emit);
+  if ((st = ds::scan_counts_permuted(emit, iota, (uint32_t)n, offs, total32, total, 0xffffffffu,
+                                     status, f->rb.scan, s)))
+    return fail(st);
+  unsigned long long h_total = 0;
+  if ((st = ds::cuda_status(cudaMemcpyAsync(&h_total, total, 8, cudaMemcpyDeviceToHost, s))) ||
+      (st = ds::cuda_status(cudaStreamSynchronize(s))))
+    return fail(st);
+  if (h_total == 0 || h_total > (unsigned long long)f->capacity) return fail(DS_ERR_OOM);
+  const int n2 = (int)h_total;
+  const size_t floats = (size_t)n2 * (14 + 3 * f->bands);
+  if ((st = ds::cuda_status(cudaMalloc(&np, floats * 4))) ||
+      (st = ds::cuda_status(cudaMalloc(&nm, floats * 4))) ||
+      (st = ds::cuda_status(cudaMalloc(&nv, floats * 4))))
+    return fail(st);
+  ds_gaussian3d Q, MQ, VQ;
+  ds::carve(np, n2, f->bands, Q);
+  ds::carve(nm, n2, f->bands, MQ);
+  ds::carve(nv, n2, f->bands, VQ);
+  ds::densify_scatter_kernel<<<blocks, ds::kThreads, 0, s>>>(f->P, f->M, f->V, mode, offs, Q, MQ,
+                                                             VQ, p->seed);
+  uint32_t nn = (uint32_t)n2;
+  if ((st = ds::cuda_status(cudaGetLastError())) ||
+      (st = ds::cuda_status(cudaMemcpyAsync(&f->rb.scalars->n_splats, &nn, 4,
+                                            cudaMemcpyHostToDevice, s))) ||
+      (st = ds::cuda_status(cudaMemsetAsync(f->grad_accum, 0, (size_t)f->capacity * 4, s))) ||
+      (st = ds::cuda_status(cudaMemsetAsync(f->grad_count, 0, (size_t)f->capacity * 4, s))) ||
+      (st = ds::cuda_status(cudaStreamSynchronize(s))))
+    return fail(st);
+  // swap in the new parameter set; the next step recaptures the graph
+  cudaFree(f->params_mem);
+  cudaFree(f->m_mem);
+  cudaFree(f->v_mem);
+  f->params_mem = np;
+  f->m_mem = nm;
+  f->v_mem = nv;
+  np = nm = nv = nullptr;
+  f->P = Q;
+  f->M = MQ;
+  f->V = VQ;
+  f->G = Q;
+  f->floats = floats;
+  f->cfg.count = n2;
+  if (f->exec) cudaGraphExecDestroy(f->exec);
+  if (f->graph) cudaGraphDestroy(f->graph);
+  f->exec = nullptr;
+  f->graph = nullptr;
+  cleanup();
+  *new_count = n2;
+  return DS_OK;
+}
+
+int ds_fitter_density_stats(ds_fitter* f, float** grad_accum, uint32_t** visible_steps) {
+  if (!f || !grad_accum || !visible_steps) return DS_ERR_ARG;
+  if (!f->grad_accum) return DS_ERR_STATE;
+  *grad_accum = f->grad_accum;
+  *visible_steps = f->grad_count;
   return DS_OK;
 }
 

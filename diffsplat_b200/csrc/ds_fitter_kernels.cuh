@@ -141,7 +141,10 @@ __global__ void __launch_bounds__(kThreads)
                              int keep_grads, int exact, int degree, const Camera* __restrict__ camp,
                              const float* __restrict__ g2sum, const float2* __restrict__ bcp,
                              const DevScalars* __restrict__ sc, Lrs lr, AdamHyper h,
-                             const uint16_t* __restrict__ inst_of_splat = nullptr) {
+                             const uint16_t* __restrict__ inst_of_splat = nullptr,
+                             const uint32_t* __restrict__ visible = nullptr,
+                             float* __restrict__ grad_accum = nullptr,
+                             uint32_t* __restrict__ grad_count = nullptr) {
   constexpr bool kBf16 = sizeof(T) == 2;
   __shared__ Mat4 sP;
   __shared__ float sCam[3];
@@ -164,6 +167,11 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int k = 0; k < 9; ++k) g2[k] = g2sum[(size_t)k * n + i];
   // g2 = {color r, g, b, ndc x, ndc y, cov2 xx, xy, yy, opacity}
+  if (grad_accum && visible[i] > 0u) {
+    // densification statistics: norm of the NDC position gradient, steps visible
+    grad_accum[i] += sqrtf(g2[3] * g2[3] + g2[4] * g2[4]);
+    grad_count[i] += 1u;
+  }
 
   // 2) projection backward (persp_project_layer.cu:245-305)
   const float px = P.pos_x[i], py = P.pos_y[i], pz = P.pos_z[i];

@@ -225,6 +225,7 @@ typedef struct ds_fitter_config {
   int32_t use_graph; /* 1: capture the step into a CUDA graph on first use */
   int32_t grad_mode; /* DS_GRAD_REFERENCE (default) / DS_GRAD_EXACT */
   int32_t schedule;  /* DS_SCHEDULE_LONGEST_FIRST (default) / DS_SCHEDULE_RASTER */
+  int32_t capacity;  /* > count: room for densification (ds_fitter_densify); 0 = count */
 } ds_fitter_config;
 
 int ds_fitter_default_config(ds_fitter_config *cfg);
@@ -271,6 +272,28 @@ int ds_fitter_counters(ds_fitter *f, uint64_t *out, int n);
 int ds_fitter_pair_stats(ds_fitter *f, uint64_t *out, int n, ds_stream stream);
 int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
 int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
+
+/* Adaptive density control (no reference counterpart: a TODO of the reference,
+ * README.md:10).  A fitter created with capacity > count accumulates, per
+ * splat, the norm of its NDC position gradient over the steps in which it was
+ * visible.  ds_fitter_densify then rebuilds the splat set in one pass:
+ * splats with opacity < min_opacity are pruned; splats whose mean gradient
+ * norm is >= grad_threshold are cloned (largest scale <= scale_threshold,
+ * world units) or split into two children sampled from their Gaussian with
+ * scales / 1.6 (larger ones); survivors keep their Adam moments, new splats
+ * start from zero moments; the statistics restart.  The count may not exceed
+ * the capacity (DS_ERR_OOM, nothing changed).  FP32 storage, without
+ * gradient inspection.  The next step recaptures the graph. */
+typedef struct ds_densify_params {
+  float grad_threshold;
+  float scale_threshold;
+  float min_opacity;
+  uint32_t seed;
+} ds_densify_params;
+int ds_fitter_densify(ds_fitter *f, const ds_densify_params *p, int32_t *new_count,
+                      ds_stream stream);
+/* Device views of the statistics [count]: gradient-norm sums and visible steps. */
+int ds_fitter_density_stats(ds_fitter *f, float **grad_accum, uint32_t **visible_steps);
 
 /* ---- Batched fitting (no reference counterpart) ----
  * Many independent ImageFitter-style instances of uneven image size and splat

@@ -39,7 +39,8 @@ def test_ctypes_struct_layouts_match_header(tmp_path):
     from diffsplat_b200 import _lib as L
     structs = {"ds_gaussian3d": L.Gaussian3D, "ds_splat3d": L.Splat3D, "ds_splat2d": L.Splat2D,
                "ds_adam_group": L.AdamGroup, "ds_fitter_config": L.FitterConfig,
-               "ds_batch_config": L.BatchConfig, "ds_batch_instance": L.BatchInstance}
+               "ds_batch_config": L.BatchConfig, "ds_batch_instance": L.BatchInstance,
+               "ds_densify_params": L.DensifyParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "diffsplat_b200.h"',
              "int main(void) {"]
     expect = []
