@@ -130,8 +130,11 @@ def fp32_peak_tflops(sm_mhz: float) -> float:
 FLOPS_PER_PAIR = {"composite_fwd": 24, "composite_bwd": 70}
 
 # DRAM bytes (read + write) per (tile, splat) pair of one composite launch, from
-# an ncu capture of the same 1280x720 / 60000-splat workload, scaled by pairs.
-NCU_DRAM_BYTES_PER_ISECT = {}
+# one ncu capture of the same 1280x720 / 60000-splat workload (profile run, step
+# 21, 3,085,549 pairs: forward 19.42 MB, backward 186.35 MB), scaled by the
+# bench's own pair count.
+NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 19.419648e6 / 3085549,
+                            "composite_bwd": 186.352896e6 / 3085549}
 
 
 def kernels_per_step(tiles: int) -> int:
