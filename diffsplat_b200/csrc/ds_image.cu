@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
 #include <cmath>
 #include <fstream>
 #include <string>
@@ -440,13 +441,13 @@ void chunk(std::vector<uint8_t>& out, const char* type, const std::vector<uint8_
 
 extern "C" {
 
-int ds_image_probe(const char* path, int* width, int* height) {
+static int ds_image_probe_impl(const char* path, int* width, int* height) {
   if (!width || !height) return DS_ERR_ARG;
   std::vector<uint8_t> rgb;
   return decode_any(path, width, height, &rgb) ? DS_OK : DS_ERR_ARG;
 }
 
-int ds_image_read_rgb8(const char* path, uint8_t* rgb, int64_t capacity, int* width,
+static int ds_image_read_rgb8_impl(const char* path, uint8_t* rgb, int64_t capacity, int* width,
                        int* height) {
   if (!rgb || !width || !height) return DS_ERR_ARG;
   std::vector<uint8_t> img;
@@ -477,7 +478,7 @@ int ds_image_fit(const uint8_t* src_rgb, int src_w, int src_h, int canvas_w, int
   return ds::cuda_status(cudaGetLastError());
 }
 
-int ds_image_write_png(const char* path, const float* rgb, int width, int height) {
+static int ds_image_write_png_impl(const char* path, const float* rgb, int width, int height) {
   if (!path || !rgb || width <= 0 || height <= 0) return DS_ERR_ARG;
   std::vector<uint8_t> raw;
   raw.reserve((size_t)(width * 3 + 1) * height);
@@ -519,6 +520,37 @@ int ds_image_write_png(const char* path, const float* rgb, int width, int height
   if (!out) return DS_ERR_ARG;
   out.write((const char*)png.data(), (std::streamsize)png.size());
   return out.good() ? DS_OK : DS_ERR_ARG;
+}
+
+// C++ exceptions (allocation, malformed numbers) become status codes at the ABI.
+int ds_image_probe(const char* path, int* width, int* height) {
+  try {
+    return ds_image_probe_impl(path, width, height);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
+}
+
+int ds_image_read_rgb8(const char* path, uint8_t* rgb, int64_t capacity, int* width, int* height) {
+  try {
+    return ds_image_read_rgb8_impl(path, rgb, capacity, width, height);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
+}
+
+int ds_image_write_png(const char* path, const float* rgb, int width, int height) {
+  try {
+    return ds_image_write_png_impl(path, rgb, width, height);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
 }
 
 }  // extern "C"

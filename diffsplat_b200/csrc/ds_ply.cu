@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
 #include <cmath>
 #include <fstream>
 #include <sstream>
@@ -87,7 +88,7 @@ int degree_of(const std::vector<std::string>& props, int* bands) {
 
 extern "C" {
 
-int ds_ply_probe(const char* path, int64_t* count, int* sh_degree) {
+static int ds_ply_probe_impl(const char* path, int64_t* count, int* sh_degree) {
   if (!path || !count || !sh_degree || !ends_with_ply(path)) return DS_ERR_ARG;
   std::ifstream f(path, std::ios::binary);
   if (!f.is_open()) return DS_ERR_ARG;
@@ -98,7 +99,7 @@ int ds_ply_probe(const char* path, int64_t* count, int* sh_degree) {
   return DS_OK;
 }
 
-int ds_ply_read(const char* path, float* splats, int64_t capacity, int64_t* count,
+static int ds_ply_read_impl(const char* path, float* splats, int64_t capacity, int64_t* count,
                 int* sh_degree) {
   if (!path || !splats || !count || !sh_degree || !ends_with_ply(path)) return DS_ERR_ARG;
   std::ifstream f(path, std::ios::binary);
@@ -147,7 +148,7 @@ int ds_ply_read(const char* path, float* splats, int64_t capacity, int64_t* coun
   return DS_OK;
 }
 
-int ds_ply_write(const char* path, const float* splats, int64_t count, int sh_num_bands) {
+static int ds_ply_write_impl(const char* path, const float* splats, int64_t count, int sh_num_bands) {
   if (!path || (!splats && count > 0) || count < 0) return DS_ERR_ARG;
   if (sh_num_bands != 0 && sh_num_bands != 3 && sh_num_bands != 8 && sh_num_bands != 15)
     return DS_ERR_ARG;
@@ -207,6 +208,37 @@ int ds_normalize_scene(float* splats, int64_t count, float scene_scale) {
     }
   }
   return DS_OK;
+}
+
+// C++ exceptions (allocation, malformed numbers) become status codes at the ABI.
+int ds_ply_probe(const char* path, int64_t* count, int* sh_degree) {
+  try {
+    return ds_ply_probe_impl(path, count, sh_degree);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
+}
+
+int ds_ply_read(const char* path, float* splats, int64_t capacity, int64_t* count, int* sh_degree) {
+  try {
+    return ds_ply_read_impl(path, splats, capacity, count, sh_degree);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
+}
+
+int ds_ply_write(const char* path, const float* splats, int64_t count, int sh_num_bands) {
+  try {
+    return ds_ply_write_impl(path, splats, count, sh_num_bands);
+  } catch (const std::bad_alloc&) {
+    return DS_ERR_OOM;
+  } catch (...) {
+    return DS_ERR_ARG;
+  }
 }
 
 }  // extern "C"
