@@ -141,6 +141,14 @@ __device__ __forceinline__ bool ellipse_hits(const float4& a, const float4& b, f
   return 0.5f * m <= cut;
 }
 
+// One splat of a batch, loaded into registers a batch ahead of its use so the
+// gathers overlap the current batch's compositing.
+struct Staged {
+  float4 a, b, c;
+  float idet;
+  bool ok;
+};
+
 // Bit w set: the splat can reach warp w's pixel block.
 template <int NW>
 __device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4& b, float cut,
@@ -190,23 +198,41 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
     done[k] = !m.inside[k];
     all_done = all_done && done[k];
   }
+  constexpr int R = (kFwdBatch + NT - 1) / NT;  // splats each thread stages
+  Staged pf[R];
+  auto prefetch = [&](int b0) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int l = threadIdx.x + r * NT, idx = b0 + l;
+      pf[r].ok = l < kFwdBatch && idx < end;
+      if (pf[r].ok) {
+        const uint32_t g = sorted_splat[idx];
+        pf[r].a = ra[g];
+        pf[r].b = rb[g];
+        pf[r].c = rc[g];
+      }
+    }
+  };
+  prefetch(start);
   for (int b0 = start; b0 < end; b0 += kFwdBatch) {
     if (__syncthreads_count(all_done) >= NT) break;
     // Stage the batch; each splat's warp-overlap mask is computed once here
     // so that every warp walks only the splats that can touch its pixels.
-    for (int l = threadIdx.x; l < kFwdBatch; l += NT) {
-      const int idx = b0 + l;
-      uint32_t mk = 0u;
-      if (idx < end) {
-        const uint32_t g = sorted_splat[idx];
-        const float4 a = ra[g], bb = rb[g], cc = rc[g];
-        sA[l] = a;
-        sB[l] = bb;
-        sC[l] = cc;
-        mk = warp_hits<NW>(a, bb, cc.w, sBox);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int l = threadIdx.x + r * NT;
+      if (l < kFwdBatch) {
+        uint32_t mk = 0u;
+        if (pf[r].ok) {
+          sA[l] = pf[r].a;
+          sB[l] = pf[r].b;
+          sC[l] = pf[r].c;
+          mk = warp_hits<NW>(pf[r].a, pf[r].b, pf[r].c.w, sBox);
+        }
+        sMask[l] = mk;
       }
-      sMask[l] = mk;
     }
+    if (b0 + kFwdBatch < end) prefetch(b0 + kFwdBatch);
     __syncthreads();
     const int bs = min(kFwdBatch, end - b0);
     bool stop = !__any_sync(0xffffffffu, !all_done);
@@ -368,25 +394,46 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
   }
   const int32_t warp_final = warp_max(my_final);
   const int nb = (end - start + B - 1) / B;
+  constexpr int R = (B + NT - 1) / NT;  // splats each thread stages
+  Staged pf[R];
+  // batch bi holds sorted indices end - 1 - B bi down to end - B (bi + 1)
+  auto prefetch = [&](int bi) {
+    const int batch_end = end - 1 - B * bi;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int l = threadIdx.x + r * NT, li = batch_end - l;
+      pf[r].ok = l < B && li >= start;
+      if (pf[r].ok) {
+        const uint32_t g = sorted_splat[li];
+        pf[r].a = ra[g];
+        pf[r].b = rb[g];
+        pf[r].c = rc[g];
+        pf[r].idet = ridet[g];
+      }
+    }
+  };
+  prefetch(0);
   for (int bi = 0; bi < nb; ++bi) {
     const int batch_end = end - 1 - B * bi;  // farthest splat of the batch
     const int bs = min(B, batch_end + 1 - start);
     __syncthreads();
     // stage the batch back to front: slot l holds sorted index batch_end - l
-    for (int l = threadIdx.x; l < B; l += NT) {
-      const int li = batch_end - l;
-      uint32_t mk = 0u;
-      if (li >= start) {
-        const uint32_t g = sorted_splat[li];
-        const float4 a = ra[g], bb = rb[g], cc = rc[g];
-        sA[l] = a;
-        sB[l] = bb;
-        sC[l] = cc;
-        sI[l] = ridet[g];
-        mk = warp_hits<NW>(a, bb, cc.w, sBox);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int l = threadIdx.x + r * NT;
+      if (l < B) {
+        uint32_t mk = 0u;
+        if (pf[r].ok) {
+          sA[l] = pf[r].a;
+          sB[l] = pf[r].b;
+          sC[l] = pf[r].c;
+          sI[l] = pf[r].idet;
+          mk = warp_hits<NW>(pf[r].a, pf[r].b, pf[r].c.w, sBox);
+        }
+        sMask[l] = mk;
       }
-      sMask[l] = mk;
     }
+    if (bi + 1 < nb) prefetch(bi + 1);
     {
       float4* p4 = reinterpret_cast<float4*>(&part[0][0]);
       for (int q = threadIdx.x; q < NW * B * 9 / 4; q += NT) p4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
