@@ -31,6 +31,12 @@ namespace ds {
 namespace {
 
 constexpr int kFwdBatch = 256;  // splats staged in shared memory per forward batch
+#ifndef DS_FWD_MIN_BLOCKS
+#define DS_FWD_MIN_BLOCKS 5
+#endif
+#ifndef DS_BWD_MIN_BLOCKS
+#define DS_BWD_MIN_BLOCKS 4
+#endif
 
 template <int PPT, int TS>
 struct Lay {
@@ -42,6 +48,9 @@ struct Lay {
   static constexpr int kWarpsX = TS / BW;
   // backward batch: the per-warp partials (kWarps x kBwdBatch x 36 B) stay within 36 KB
   static constexpr int kBwdBatch = 1024 / kWarps < 128 ? 1024 / kWarps : 128;
+  // resident CTAs per SM the register allocation must allow (256-thread CTAs)
+  static constexpr int kMinBlocksFwd = kThreads == 256 ? DS_FWD_MIN_BLOCKS : 1;
+  static constexpr int kMinBlocksBwd = kThreads == 256 ? DS_BWD_MIN_BLOCKS : 1;
   static_assert(kThreads % 32 == 0 && BW <= TS && kWarps <= 32, "unsupported tile layout");
 };
 
@@ -160,7 +169,7 @@ __device__ __forceinline__ uint32_t warp_hits(const float4& a, const float4& b, 
 }
 
 template <int PPT, int TS, bool kLoss, bool kCount, bool kBatch>
-__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
+__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBlocksFwd)
     composite_fwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const uint32_t* __restrict__ sorted_splat,
                          const int2* __restrict__ ranges, const int32_t* __restrict__ order,
@@ -339,7 +348,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
 }
 
 template <int PPT, int TS, bool kFusedLoss, bool kExact, bool kBatch>
-__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads)
+__global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBlocksBwd)
     composite_bwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const float* __restrict__ ridet,
                          const uint32_t* __restrict__ sorted_splat,
