@@ -109,13 +109,13 @@ static int batch_enqueue(ds_batch* b, cudaStream_t s) {
   if (bf16) batch_preprocess(b, b->R16, s);
   else batch_preprocess(b, soa_of(b->P), s);
   DS_CUDA(cudaGetLastError());
-  DS_TRY(raster_build_lists(rb, n, s));
+  DS_TRY(raster_build_lists(rb, n, s, nullptr, true));
   DS_TRY(raster_composite_forward(rb, b->images, b->targets, s));
   batch_loss_kernel<<<(b->instances * 32 + 255) / 256, 256, 0, s>>>(
       rb.loss_partials, b->geom_dev, b->instances, b->losses);
   DS_CUDA(cudaGetLastError());
   DS_TRY(raster_composite_backward(rb, b->images, nullptr, b->targets, s));
-  DS_TRY(raster_reduce_grads_soa(rb, n, s));
+  DS_TRY(raster_reduce_long_grads(rb, n, s));
   Lrs lr{b->cfg.lr_pos, b->cfg.lr_scale, b->cfg.lr_rot, b->cfg.lr_sh_dc, b->cfg.lr_sh_rest,
          b->cfg.lr_opacity};
   AdamHyper h{b->cfg.beta1, b->cfg.beta2, b->cfg.epsilon};
@@ -124,12 +124,12 @@ static int batch_enqueue(ds_batch* b, cudaStream_t s) {
   ds_gaussian3d G = b->P;  // unused: keep_grads == 0
   if (bf16)
     fit_backward_adam_kernel<__nv_bfloat16, true><<<blocks, kThreads, 0, s>>>(
-        b->P, b->R16, b->M16, b->V16, G, 0, exact, b->cfg.sh_degree, b->cams, rb.g2, b->bc_cur,
-        rb.scalars, lr, h, b->inst_of_splat);
+        b->P, b->R16, b->M16, b->V16, G, 0, exact, b->cfg.sh_degree, b->cams, rb.g2,
+        grad_segments(rb), b->bc_cur, rb.scalars, lr, h, b->inst_of_splat);
   else
     fit_backward_adam_kernel<float, true><<<blocks, kThreads, 0, s>>>(
         b->P, soa_of(b->P), soa_of(b->M), soa_of(b->V), G, 0, exact, b->cfg.sh_degree, b->cams,
-        rb.g2, b->bc_cur, rb.scalars, lr, h, b->inst_of_splat);
+        rb.g2, grad_segments(rb), b->bc_cur, rb.scalars, lr, h, b->inst_of_splat);
   return cuda_status(cudaGetLastError());
 }
 

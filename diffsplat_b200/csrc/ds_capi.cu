@@ -159,7 +159,7 @@ int ds_raster_forward(ds_raster* r, const ds_splat2d* in, float* out_rgb, ds_str
   if (!r || !s2_ok(in) || !out_rgb || in->count > r->rb.max_splats) return DS_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   DS_TRY(ds::raster_prepare_from_splat2d(r->rb, *in, s));
-  DS_TRY(ds::raster_build_lists(r->rb, in->count, s));
+  DS_TRY(ds::raster_build_lists(r->rb, in->count, s, nullptr, true));
   DS_TRY(ds::raster_composite_forward(r->rb, out_rgb, nullptr, s));
   r->last_count = in->count;
   return DS_OK;

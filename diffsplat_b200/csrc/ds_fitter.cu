@@ -84,12 +84,12 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
         rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
-  DS_TRY(raster_build_lists(rb, n, s, ev ? ev + 2 : nullptr));
+  DS_TRY(raster_build_lists(rb, n, s, ev ? ev + 2 : nullptr, true));
   DS_TRY(raster_composite_forward(rb, f->image, f->target, s));
   if (ev) DS_CUDA(cudaEventRecord(ev[5], s));
   DS_TRY(raster_composite_backward(rb, f->image, nullptr, f->target, s));
   if (ev) DS_CUDA(cudaEventRecord(ev[6], s));
-  DS_TRY(raster_reduce_grads_soa(rb, n, s));
+  DS_TRY(raster_reduce_long_grads(rb, n, s));
   Lrs lr{f->cfg.lr_pos, f->cfg.lr_scale, f->cfg.lr_rot, f->cfg.lr_sh_dc, f->cfg.lr_sh_rest,
          f->cfg.lr_opacity};
   AdamHyper h{f->cfg.beta1, f->cfg.beta2, f->cfg.epsilon};
@@ -97,12 +97,13 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   if (bf16)
     fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
         f->P, f->R16, f->M16, f->V16, f->G, keep, exact, f->cfg.sh_degree, f->cam_dev, rb.g2,
-        f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum, f->grad_count);
+        grad_segments(rb), f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum,
+        f->grad_count);
   else
     fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
         f->P, soa_of(f->P), soa_of(f->M), soa_of(f->V), f->G, keep, exact, f->cfg.sh_degree,
-        f->cam_dev, rb.g2, f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum,
-        f->grad_count);
+        f->cam_dev, rb.g2, grad_segments(rb), f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts,
+        f->grad_accum, f->grad_count);
   DS_CUDA(cudaGetLastError());
   if (ev) DS_CUDA(cudaEventRecord(ev[7], s));
   return DS_OK;

@@ -139,7 +139,8 @@ template <typename T, bool kBatch = false>
 __global__ void __launch_bounds__(kThreads)
     fit_backward_adam_kernel(ds_gaussian3d P, Soa<T> R, Soa<T> M, Soa<T> V, ds_gaussian3d G,
                              int keep_grads, int exact, int degree, const Camera* __restrict__ camp,
-                             const float* __restrict__ g2sum, const float2* __restrict__ bcp,
+                             const float* __restrict__ g2sum, GradSegments seg,
+                             const float2* __restrict__ bcp,
                              const DevScalars* __restrict__ sc, Lrs lr, AdamHyper h,
                              const uint16_t* __restrict__ inst_of_splat = nullptr,
                              const uint32_t* __restrict__ visible = nullptr,
@@ -162,10 +163,31 @@ __global__ void __launch_bounds__(kThreads)
   const float2 bc = *bcp;
   const uint32_t step = kBf16 ? sc->step : 0u;
 
-  // 1) Splat2D gradient = sum of this splat's per-tile records (segment_reduce_kernel).
+  // 1) Splat2D gradient = sum of this splat's per-tile records: summed here in
+  // record order when it has at most kSerialRecords tiles, else read from the
+  // long-segment reduction (segment_reduce_long_kernel).
   float g2[9];
+  {
+    const uint32_t c = seg.counts[i];
+    unsigned long long s0 = 0, e0 = 0;
+    if (c) {
+      s0 = seg.start[i];
+      e0 = s0 + c;
+      if (e0 > seg.cap) e0 = seg.cap;
+    }
+    if (c > kSerialRecords) {
 #pragma unroll
-  for (int k = 0; k < 9; ++k) g2[k] = g2sum[(size_t)k * n + i];
+      for (int k = 0; k < 9; ++k) g2[k] = g2sum[(size_t)k * n + i];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) g2[k] = 0.f;
+      for (unsigned long long q = s0; q < e0; ++q) {
+        const float* r = seg.rec + q * 9;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g2[k] += r[k];
+      }
+    }
+  }
   // g2 = {color r, g, b, ndc x, ndc y, cov2 xx, xy, yy, opacity}
   if (grad_accum && visible[i] > 0u) {
     // densification statistics: norm of the NDC position gradient, steps visible
@@ -263,37 +285,87 @@ __global__ void __launch_bounds__(kThreads)
 
   // 4) Adam on every field (adam.cu:12-37), group learning rates of
   //    registerGaussian3DGroups (gaussian3d_adam.h:27-55).  In BF16 storage
-  //    the render copy of every non-position field follows its master.
+  //    the render copy of every non-position field follows its master.  All
+  //    loads of a group of fields are issued before its first store (the
+  //    arrays could alias as far as the compiler knows), so they overlap.
   const float b1 = h.b1, b2 = h.b2, eps = h.eps, bc1 = bc.x, bc2 = bc.y;
-  uint32_t field = 0;
-  auto upd = [&](float* p, T* m, T* vv, T* r, int64_t k, float g, float l) {
-    adam_at(p, m, vv, k, g, l, b1, b2, eps, bc1, bc2, mix32(step * 32u + field++));
-    if (kBf16 && r) r[k] = __float2bfloat16_rn(p[k]);
+  const uint32_t salt = step * 0x85ebca6bu;
+  auto finish = [&](float* p, T* m, T* vv, T* r, int64_t k, uint32_t field, float pk, float mk,
+                    float vk, float g, float l) {
+    adam1(pk, mk, vk, g, l, b1, b2, eps, bc1, bc2);
+    p[k] = pk;
+    // one hash per element: its low 16 bits round m, its high 16 bits round v
+    const uint32_t hs = mix32((uint32_t)k * 0x9e3779b1u ^ salt ^ field * 0xc2b2ae35u);
+    store_moment(m + k, mk, hs);
+    store_moment(vv + k, vk, hs >> 16);
+    if (kBf16 && r) r[k] = __float2bfloat16_rn(pk);
   };
-  upd(P.pos_x, M.pos_x, V.pos_x, nullptr, i, gpos[0], lr.pos);
-  upd(P.pos_y, M.pos_y, V.pos_y, nullptr, i, gpos[1], lr.pos);
-  upd(P.pos_z, M.pos_z, V.pos_z, nullptr, i, gpos[2], lr.pos);
-  upd(P.scale_x, M.scale_x, V.scale_x, R.scale_x, i, d[0], lr.scale);
-  upd(P.scale_y, M.scale_y, V.scale_y, R.scale_y, i, d[1], lr.scale);
-  upd(P.scale_z, M.scale_z, V.scale_z, R.scale_z, i, d[2], lr.scale);
-  upd(P.rot_w, M.rot_w, V.rot_w, R.rot_w, i, d[3], lr.rot);
-  upd(P.rot_x, M.rot_x, V.rot_x, R.rot_x, i, d[4], lr.rot);
-  upd(P.rot_y, M.rot_y, V.rot_y, R.rot_y, i, d[5], lr.rot);
-  upd(P.rot_z, M.rot_z, V.rot_z, R.rot_z, i, d[6], lr.rot);
-  upd(P.sh_dc_r, M.sh_dc_r, V.sh_dc_r, R.sh_dc_r, i, dR * kC0, lr.sh_dc);
-  upd(P.sh_dc_g, M.sh_dc_g, V.sh_dc_g, R.sh_dc_g, i, dG * kC0, lr.sh_dc);
-  upd(P.sh_dc_b, M.sh_dc_b, V.sh_dc_b, R.sh_dc_b, i, dB * kC0, lr.sh_dc);
-  upd(P.logit_opacity, M.logit_opacity, V.logit_opacity, R.logit_opacity, i, glogit,
-      lr.opacity);
+  {
+    float* pf[14] = {P.pos_x,   P.pos_y,   P.pos_z,   P.scale_x, P.scale_y,
+                     P.scale_z, P.rot_w,   P.rot_x,   P.rot_y,   P.rot_z,
+                     P.sh_dc_r, P.sh_dc_g, P.sh_dc_b, P.logit_opacity};
+    T* mf[14] = {M.pos_x,   M.pos_y,   M.pos_z,   M.scale_x, M.scale_y,
+                 M.scale_z, M.rot_w,   M.rot_x,   M.rot_y,   M.rot_z,
+                 M.sh_dc_r, M.sh_dc_g, M.sh_dc_b, M.logit_opacity};
+    T* vf[14] = {V.pos_x,   V.pos_y,   V.pos_z,   V.scale_x, V.scale_y,
+                 V.scale_z, V.rot_w,   V.rot_x,   V.rot_y,   V.rot_z,
+                 V.sh_dc_r, V.sh_dc_g, V.sh_dc_b, V.logit_opacity};
+    T* rf[14] = {nullptr,   nullptr,   nullptr,   R.scale_x, R.scale_y,
+                 R.scale_z, R.rot_w,   R.rot_x,   R.rot_y,   R.rot_z,
+                 R.sh_dc_r, R.sh_dc_g, R.sh_dc_b, R.logit_opacity};
+    const float g[14] = {gpos[0], gpos[1], gpos[2], d[0],     d[1],     d[2],     d[3],
+                         d[4],    d[5],    d[6],    dR * kC0, dG * kC0, dB * kC0, glogit};
+    const float lf[14] = {lr.pos, lr.pos, lr.pos, lr.scale, lr.scale, lr.scale,  lr.rot,
+                          lr.rot, lr.rot, lr.rot, lr.sh_dc, lr.sh_dc, lr.sh_dc, lr.opacity};
+    float pp[14], mm[14], vv[14];
+#pragma unroll
+    for (int k = 0; k < 14; ++k) {
+      pp[k] = pf[k][i];
+      mm[k] = ldv(mf[k][i]);
+      vv[k] = ldv(vf[k][i]);
+    }
+#pragma unroll
+    for (int k = 0; k < 14; ++k)
+      finish(pf[k], mf[k], vf[k], rf[k], i, (uint32_t)k, pp[k], mm[k], vv[k], g[k], lf[k]);
+  }
   const int nb = P.sh_num_bands;
   const int nb_used = sh_bands(degree);
-  for (int b = 0; b < nb; ++b) {
-    const int64_t k = (int64_t)b * n + i;
-    const float yb = b < nb_used ? y[b] : 0.f;
-    field = 16u + 3u * (uint32_t)b;
-    upd(P.sh_rest_r, M.sh_rest_r, V.sh_rest_r, R.sh_rest_r, k, dR * yb, lr.sh_rest);
-    upd(P.sh_rest_g, M.sh_rest_g, V.sh_rest_g, R.sh_rest_g, k, dG * yb, lr.sh_rest);
-    upd(P.sh_rest_b, M.sh_rest_b, V.sh_rest_b, R.sh_rest_b, k, dB * yb, lr.sh_rest);
+  if (nb > 0) {
+    float* pr[3] = {P.sh_rest_r, P.sh_rest_g, P.sh_rest_b};
+    T* mr[3] = {M.sh_rest_r, M.sh_rest_g, M.sh_rest_b};
+    T* vr[3] = {V.sh_rest_r, V.sh_rest_g, V.sh_rest_b};
+    T* rr[3] = {R.sh_rest_r, R.sh_rest_g, R.sh_rest_b};
+    const float dc[3] = {dR, dG, dB};
+    float cp[3], cm[3], cv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cp[c] = pr[c][i];
+      cm[c] = ldv(mr[c][i]);
+      cv[c] = ldv(vr[c][i]);
+    }
+    for (int b = 0; b < nb; ++b) {
+      // band b + 1 is loaded before band b is stored
+      float np[3] = {0.f, 0.f, 0.f}, nm[3] = {0.f, 0.f, 0.f}, nv[3] = {0.f, 0.f, 0.f};
+      if (b + 1 < nb) {
+        const int64_t k1 = (int64_t)(b + 1) * n + i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          np[c] = pr[c][k1];
+          nm[c] = ldv(mr[c][k1]);
+          nv[c] = ldv(vr[c][k1]);
+        }
+      }
+      const int64_t k = (int64_t)b * n + i;
+      const float yb = b < nb_used ? y[b] : 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        finish(pr[c], mr[c], vr[c], rr[c], k, 16u + 3u * (uint32_t)b + (uint32_t)c, cp[c], cm[c],
+               cv[c], dc[c] * yb, lr.sh_rest);
+        cp[c] = np[c];
+        cm[c] = nm[c];
+        cv[c] = nv[c];
+      }
+    }
   }
 }
 

@@ -59,13 +59,24 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
 //   offsets[p] = sum_{q < p} counts[perm[q]]   (64-bit),
 //   *raw_total = the full sum, *n_clamped = min(raw_total, cap), and the
 //   overflow bit is or-ed into *status when raw_total > cap.
+// Gradient records of a splat's tiles are contiguous in emission order.  A
+// splat with at most kSerialRecords tiles has its records summed by one thread
+// in record order; one with more by a warp (lane-strided partial sums, then a
+// tree), taken from the list of those splats that the emission scan writes.
+constexpr uint32_t kSerialRecords = 8;
+
 struct ScanScratch {
   unsigned long long* partials = nullptr;  // [kSortBlocks + 1]
+  uint32_t* long_partials = nullptr;       // [kSortBlocks]; only for the long list
 };
+// offsets[p] = exclusive sum of counts[perm[q]], q < p.  With long_list set,
+// also long_list[0 .. *n_long) = the positions p with counts[perm[p]] >
+// kSerialRecords, ascending.
 int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
                          unsigned long long* offsets, uint32_t* n_clamped,
                          unsigned long long* raw_total, uint32_t cap, uint32_t* status,
-                         ScanScratch& scratch, cudaStream_t s);
+                         ScanScratch& scratch, cudaStream_t s, uint32_t* long_list = nullptr,
+                         uint32_t* n_long = nullptr);
 
 // Device-resident scalars of one rasterizer / fitter.
 struct DevScalars {
@@ -75,7 +86,8 @@ struct DevScalars {
   uint32_t ticket;    // CTA-completion counter of the fused loss reduction
   uint32_t n_splats;  // element count of the depth sort
   uint32_t step;      // Adam step count (fitter)
-  uint32_t pad[2];
+  uint32_t n_long;    // splats with more than kSerialRecords tiles (last emission scan)
+  uint32_t pad;
   unsigned long long n_isects_raw;  // unclamped pair count
   float loss;
   float pad2;
@@ -118,6 +130,7 @@ struct RasterBuffers {
   ushort4* rect = nullptr;     // tile rectangle {x0, x1, y0, y1}
   uint32_t* counts = nullptr;  // tiles per splat (0 = invisible)
   uint32_t* seg_start = nullptr;  // first emission index of each splat
+  uint32_t* long_list = nullptr;  // depth-order positions of splats with long record segments
   uint32_t* depth_keys = nullptr;  // depth key of each splat (0xffffffff when invisible)
   uint32_t* depth_k0 = nullptr;    // ping-pong buffers of the depth sort
   uint32_t* depth_k1 = nullptr;
@@ -154,6 +167,18 @@ struct RasterBuffers {
   ScanScratch scan;
 };
 
+// Where a consumer finds splat i's gradient records: [start[i], start[i] +
+// counts[i]) clamped to cap, 9 floats each.
+struct GradSegments {
+  const float* rec;
+  const uint32_t* counts;
+  const uint32_t* start;
+  uint32_t cap;
+};
+inline GradSegments grad_segments(const RasterBuffers& rb) {
+  return GradSegments{rb.isect_grad, rb.counts, rb.seg_start, (uint32_t)rb.cap};
+}
+
 int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap);
 // Pixels per thread of the composite kernels; DS_COMPOSITE_PPT=1|2|4 overrides
 // the default (a tuning knob: results are identical for every value).
@@ -172,7 +197,10 @@ void raster_free(RasterBuffers& rb);
 
 // Everything after the per-splat records exist: depth sort, emission, tile
 // sort, ranges.  Records, rect, counts and depth_keys must be filled for n splats.
-int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// with_long_list: also write rb.long_list / scalars->n_long (callers that
+// reduce gradients afterwards).
+int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev = nullptr,
+                       bool with_long_list = false);
 
 // Composite forward.  When target != nullptr the per-tile squared error is
 // also accumulated and reduced into rb.scalars->loss (L = sum / pixels).
@@ -191,8 +219,10 @@ int raster_composite_backward(RasterBuffers& rb, const float* image, const float
 // Layer-API preprocess from Splat2D SoA, and reduction of isect_grad into Splat2D grads.
 int raster_prepare_from_splat2d(RasterBuffers& rb, const ds_splat2d& in, cudaStream_t s);
 int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStream_t s);
-// Same sums written (not accumulated) to rb.g2 [9][n].
-int raster_reduce_grads_soa(RasterBuffers& rb, int n, cudaStream_t s);
+// The sums of the long segments only (the splats on rb.long_list), written to
+// rb.g2[k * n + i]; the fitters' backward kernel sums the short segments
+// itself from grad_segments(rb).
+int raster_reduce_long_grads(RasterBuffers& rb, int n, cudaStream_t s);
 
 // Losses and Adam (ds_loss_adam.cu)
 int launch_mse_forward(const float* px, const float* tgt, int64_t npix, float* loss,

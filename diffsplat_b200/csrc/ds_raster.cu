@@ -16,6 +16,8 @@
 //     records here: no global atomics, deterministic gradients.
 #include <float.h>
 
+#include <algorithm>
+
 #include "ds_common.cuh"
 #include "ds_internal.h"
 
@@ -97,50 +99,107 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Sums each splat's per-tile gradient records; one warp per splat in depth
-// order, whose records are contiguous in emission order.  kAccumulate adds the
-// sums into a Splat2D gradient SoA (layer API); otherwise they are written to
-// g2[k * n + i], k = {r, g, b, ndc x, ndc y, cov xx, cov xy, cov yy, opacity}.
+// Sums each splat's per-tile gradient records, which are contiguous in
+// emission order.  One thread per splat with at most kSerialRecords tiles sums
+// them in record order; a fixed grid of warps takes the splats on the
+// emission scan's long list one per warp (grid-stride).  Each splat is summed
+// by exactly one thread or warp in a fixed order.  kAccumulate adds the sums into a Splat2D gradient SoA (layer
+// API); otherwise they are written to g2[k * n + i], k = {r, g, b, ndc x,
+// ndc y, cov xx, cov xy, cov yy, opacity}.
+constexpr int kLongWarps = 148 * 256;  // enough for one long segment per warp in typical scenes
+
+template <bool kAccumulate>
+__device__ __forceinline__ void store_g2(int k, uint32_t i, int n, float v, float* g2,
+                                         const ds_splat2d& gin) {
+  if (kAccumulate) {
+    float* dst = k == 0 ? gin.color_r : k == 1 ? gin.color_g : k == 2 ? gin.color_b
+               : k == 3 ? gin.pos_x : k == 4 ? gin.pos_y : k == 5 ? gin.cov_xx
+               : k == 6 ? gin.cov_xy : k == 7 ? gin.cov_yy : gin.opacity;
+    dst[i] += v;
+  } else {
+    g2[(size_t)k * n + i] = v;
+  }
+}
+
+__device__ __forceinline__ void segment_of(const uint32_t* __restrict__ perm,
+                                           const unsigned long long* __restrict__ offsets,
+                                           const uint32_t* __restrict__ counts, uint32_t cap,
+                                           int p, uint32_t& i, uint32_t& c,
+                                           unsigned long long& s, unsigned long long& e) {
+  i = perm[p];
+  c = counts[i];
+  s = e = 0;
+  if (c) {
+    s = offsets[p];
+    e = s + c;
+    if (e > cap) e = cap;
+    if (s > e) s = e;
+  }
+}
+
 template <bool kAccumulate>
 __global__ void __launch_bounds__(kThreads)
-    segment_reduce_kernel(const float* __restrict__ isect_grad, const uint32_t* __restrict__ perm,
-                          const unsigned long long* __restrict__ offsets,
-                          const uint32_t* __restrict__ counts, uint32_t cap, int n,
-                          float* __restrict__ g2, ds_splat2d gin) {
-  const int p = (int)((blockIdx.x * (unsigned)kThreads + threadIdx.x) >> 5);
+    segment_reduce_short_kernel(const float* __restrict__ isect_grad,
+                                const uint32_t* __restrict__ perm,
+                                const unsigned long long* __restrict__ offsets,
+                                const uint32_t* __restrict__ counts, uint32_t cap, int n,
+                                float* __restrict__ g2, ds_splat2d gin) {
+  const int p = (int)(blockIdx.x * (int64_t)kThreads + threadIdx.x);
+  if (p >= n) return;
+  uint32_t i, c;
+  unsigned long long s, e;
+  segment_of(perm, offsets, counts, cap, p, i, c, s, e);
+  if (c > kSerialRecords || (kAccumulate && c == 0)) return;
+  float v[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (unsigned long long q = s; q < e; ++q) {
+    const float* r = isect_grad + q * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] += r[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) store_g2<kAccumulate>(k, i, n, v[k], g2, gin);
+}
+
+template <bool kAccumulate>
+__global__ void __launch_bounds__(kThreads)
+    segment_reduce_long_kernel(const float* __restrict__ isect_grad,
+                               const uint32_t* __restrict__ perm,
+                               const unsigned long long* __restrict__ offsets,
+                               const uint32_t* __restrict__ counts, uint32_t cap, int n,
+                               float* __restrict__ g2, ds_splat2d gin,
+                               const uint32_t* __restrict__ long_list,
+                               DevScalars* __restrict__ sc) {
   const int lane = threadIdx.x & 31;
-  if (p >= n) return;  // uniform per warp
-  const uint32_t i = perm[p];
-  const uint32_t c = counts[i];
-  float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  float a = 0.f;
-  if (c) {
-    const unsigned long long s = offsets[p];
-    unsigned long long e = s + c;
-    if (e > cap) e = cap;
+  const uint32_t total = sc->n_long;
+  for (uint32_t w = (uint32_t)((blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5); w < total;
+       w += (uint32_t)(gridDim.x * (kThreads / 32))) {
+    uint32_t i, c;
+    unsigned long long s, e;
+    segment_of(perm, offsets, counts, cap, (int)long_list[w], i, c, s, e);
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float a = 0.f;
     for (unsigned long long q = s + lane; q < e; q += 32) {
       const float* r = isect_grad + q * 9;
 #pragma unroll
       for (int k = 0; k < 8; ++k) v[k] += r[k];
       a += r[8];
     }
+    const float s8 = warp_sum8_transposed(v, lane);
+    const float sa = warp_sum(a);
+    if ((lane & 3) == 0) store_g2<kAccumulate>(lane >> 2, i, n, s8, g2, gin);
+    if (lane == 0) store_g2<kAccumulate>(8, i, n, sa, g2, gin);
   }
-  const float s8 = warp_sum8_transposed(v, lane);
-  const float sa = warp_sum(a);
-  const int k = lane >> 2;
-  if (kAccumulate) {
-    if (c == 0) return;
-    if ((lane & 3) == 0) {
-      float* dst = k == 0 ? gin.color_r : k == 1 ? gin.color_g : k == 2 ? gin.color_b
-                 : k == 3 ? gin.pos_x : k == 4 ? gin.pos_y : k == 5 ? gin.cov_xx
-                 : k == 6 ? gin.cov_xy : gin.cov_yy;
-      dst[i] += s8;
-    }
-    if (lane == 0) gin.opacity[i] += sa;
-  } else {
-    if ((lane & 3) == 0) g2[(size_t)k * n + i] = s8;
-    if (lane == 0) g2[(size_t)8 * n + i] = sa;
-  }
+  (void)n;
+}
+
+template <bool kAccumulate>
+int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStream_t s) {
+  const int64_t warps = std::min<int64_t>(n, kLongWarps);
+  const unsigned blocks = (unsigned)((warps * 32 + kThreads - 1) / kThreads);
+  segment_reduce_long_kernel<kAccumulate><<<blocks, kThreads, 0, s>>>(
+      rb.isect_grad, rb.depth_perm, rb.emit_offsets, rb.counts, (uint32_t)rb.cap, n, rb.g2, gin,
+      rb.long_list, rb.scalars);
+  return cuda_status(cudaGetLastError());
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -262,6 +321,7 @@ static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   DS_TRY(alloc(&rb.rect, n));
   DS_TRY(alloc(&rb.counts, n));
   DS_TRY(alloc(&rb.seg_start, n));
+  DS_TRY(alloc(&rb.long_list, n));
   DS_TRY(alloc(&rb.depth_keys, n));
   DS_TRY(alloc(&rb.depth_k0, n));
   DS_TRY(alloc(&rb.depth_k1, n));
@@ -279,6 +339,7 @@ static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   DS_TRY(alloc(&rb.isect_grad, c * 9));
   DS_TRY(alloc(&rb.sort.hist, (size_t)256 * kSortBlocks));
   DS_TRY(alloc(&rb.scan.partials, (size_t)kSortBlocks + 1));
+  DS_TRY(alloc(&rb.scan.long_partials, (size_t)kSortBlocks));
   DS_TRY(alloc(&rb.scalars, 1));
   DS_CUDA(cudaMemset(rb.scalars, 0, sizeof(DevScalars)));
   // Splats that are never visible keep count 0 until the first forward writes them.
@@ -344,6 +405,7 @@ void raster_free(RasterBuffers& rb) {
   release(rb.rect);
   release(rb.counts);
   release(rb.seg_start);
+  release(rb.long_list);
   release(rb.depth_keys);
   release(rb.depth_k0);
   release(rb.depth_k1);
@@ -360,6 +422,7 @@ void raster_free(RasterBuffers& rb) {
   release(rb.isect_grad);
   release(rb.sort.hist);
   release(rb.scan.partials);
+  release(rb.scan.long_partials);
   release(rb.scalars);
   release(rb.ranges);
   release(rb.tile_order);
@@ -380,7 +443,8 @@ int raster_prepare_from_splat2d(RasterBuffers& rb, const ds_splat2d& in, cudaStr
   return cuda_status(cudaGetLastError());
 }
 
-int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev) {
+int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev,
+                       bool with_long_list) {
   DevScalars* sc = rb.scalars;
   if (n > 0) {
     // 1) depth order of the splats: stable sort of (depth bits, id)
@@ -391,7 +455,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     // 2) emission offsets in depth order
     DS_TRY(scan_counts_permuted(rb.counts, rb.depth_perm, (uint32_t)n, rb.emit_offsets,
                                 &sc->n_isects, &sc->n_isects_raw, (uint32_t)rb.cap, &sc->status,
-                                rb.scan, s));
+                                rb.scan, s, with_long_list ? rb.long_list : nullptr, &sc->n_long));
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
     emit_kernel<<<(unsigned)(((int64_t)n * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
@@ -426,21 +490,16 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
 
 int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStream_t s) {
   if (n <= 0) return DS_OK;
-  const unsigned blocks = (unsigned)(((int64_t)n * 32 + kThreads - 1) / kThreads);
-  segment_reduce_kernel<true><<<blocks, kThreads, 0, s>>>(rb.isect_grad, rb.depth_perm,
-                                                          rb.emit_offsets, rb.counts,
-                                                          (uint32_t)rb.cap, n, nullptr, gin);
-  return cuda_status(cudaGetLastError());
+  segment_reduce_short_kernel<true><<<(unsigned)(((int64_t)n + kThreads - 1) / kThreads), kThreads,
+                                      0, s>>>(rb.isect_grad, rb.depth_perm, rb.emit_offsets,
+                                              rb.counts, (uint32_t)rb.cap, n, rb.g2, gin);
+  DS_CUDA(cudaGetLastError());
+  return launch_long_reduce<true>(rb, n, gin, s);
 }
 
-int raster_reduce_grads_soa(RasterBuffers& rb, int n, cudaStream_t s) {
+int raster_reduce_long_grads(RasterBuffers& rb, int n, cudaStream_t s) {
   if (n <= 0) return DS_OK;
-  const unsigned blocks = (unsigned)(((int64_t)n * 32 + kThreads - 1) / kThreads);
-  segment_reduce_kernel<false><<<blocks, kThreads, 0, s>>>(rb.isect_grad, rb.depth_perm,
-                                                           rb.emit_offsets, rb.counts,
-                                                           (uint32_t)rb.cap, n, rb.g2,
-                                                           ds_splat2d{});
-  return cuda_status(cudaGetLastError());
+  return launch_long_reduce<false>(rb, n, ds_splat2d{}, s);
 }
 
 }  // namespace ds

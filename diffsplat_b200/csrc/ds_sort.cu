@@ -183,91 +183,150 @@ __device__ __forceinline__ uint32_t scan_chunk(uint32_t n) {
   return (per + step - 1) / step * step;
 }
 
+// With long_partials / long_list set, the same passes also count the splats
+// whose tile count exceeds kSerialRecords and write their depth-order
+// positions, in depth order, to long_list (their number to *n_long): the list
+// the long-segment gradient reduction walks.
 __global__ void __launch_bounds__(kThreads)
     scan_partial_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
-                        uint32_t n, unsigned long long* __restrict__ partials) {
+                        uint32_t n, unsigned long long* __restrict__ partials,
+                        uint32_t* __restrict__ long_partials) {
   __shared__ unsigned long long wsum[kWarps];
+  __shared__ uint32_t wlong[kWarps];
   const uint32_t chunk = scan_chunk(n);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   unsigned long long s = 0;
-  for (uint32_t p = begin + threadIdx.x; p < end; p += kThreads) s += counts[perm[p]];
+  uint32_t l = 0;
+  for (uint32_t p = begin + threadIdx.x; p < end; p += kThreads) {
+    const uint32_t c = counts[perm[p]];
+    s += c;
+    l += c > kSerialRecords ? 1u : 0u;
+  }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    wsum[threadIdx.x >> 5] = s;
+    wlong[threadIdx.x >> 5] = l;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long t = 0;
-    for (int k = 0; k < kWarps; ++k) t += wsum[k];
+    uint32_t tl = 0;
+    for (int k = 0; k < kWarps; ++k) {
+      t += wsum[k];
+      tl += wlong[k];
+    }
     partials[blockIdx.x] = t;
+    if (long_partials) long_partials[blockIdx.x] = tl;
   }
 }
 
 __global__ void __launch_bounds__(kThreads)
-    scan_partials_kernel(unsigned long long* __restrict__ partials, uint32_t cap,
+    scan_partials_kernel(unsigned long long* __restrict__ partials,
+                         uint32_t* __restrict__ long_partials, uint32_t cap,
                          uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
-                         uint32_t* __restrict__ status) {
+                         uint32_t* __restrict__ n_long, uint32_t* __restrict__ status) {
   __shared__ unsigned long long buf[kSortBlocks];
-  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) buf[i] = partials[i];
+  __shared__ uint32_t lbuf[kSortBlocks];
+  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) {
+    buf[i] = partials[i];
+    lbuf[i] = long_partials ? long_partials[i] : 0u;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long run = 0;
+    uint32_t lrun = 0;
     for (int i = 0; i < kSortBlocks; ++i) {
-      unsigned long long v = buf[i];
+      const unsigned long long v = buf[i];
+      const uint32_t lv = lbuf[i];
       buf[i] = run;
+      lbuf[i] = lrun;
       run += v;
+      lrun += lv;
     }
     *raw = run;
     *n_clamped = (uint32_t)(run < (unsigned long long)cap ? run : cap);
     if (run > (unsigned long long)cap) atomicOr(status, kStatusIsectOverflow);
+    if (n_long) *n_long = lrun;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) partials[i] = buf[i];
+  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) {
+    partials[i] = buf[i];
+    if (long_partials) long_partials[i] = lbuf[i];
+  }
 }
 
 __global__ void __launch_bounds__(kThreads)
     scan_final_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
                       uint32_t n, const unsigned long long* __restrict__ partials,
-                      unsigned long long* __restrict__ offsets) {
+                      unsigned long long* __restrict__ offsets,
+                      const uint32_t* __restrict__ long_partials,
+                      uint32_t* __restrict__ long_list) {
   __shared__ unsigned long long wsum[kWarps];
+  __shared__ uint32_t wlong[kWarps];
   const uint32_t chunk = scan_chunk(n);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
   unsigned long long carry = partials[blockIdx.x];
+  uint32_t lcarry = long_list ? long_partials[blockIdx.x] : 0u;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (uint32_t t0 = begin; t0 < end; t0 += kThreads * kScanItems) {
     uint32_t c[kScanItems];
     unsigned long long s = 0;
+    uint32_t lmask = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
       uint32_t p = t0 + threadIdx.x * kScanItems + k;
       c[k] = p < end ? counts[perm[p]] : 0u;
       s += c[k];
+      lmask |= (c[k] > kSerialRecords ? 1u : 0u) << k;
     }
+    const uint32_t ls = __popc(lmask);
     unsigned long long incl = s;
+    uint32_t lincl = ls;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+      uint32_t tl = __shfl_up_sync(0xffffffffu, lincl, o);
+      if (lane >= o) {
+        incl += t;
+        lincl += tl;
+      }
     }
-    if (lane == 31) wsum[w] = incl;
+    if (lane == 31) {
+      wsum[w] = incl;
+      wlong[w] = lincl;
+    }
     __syncthreads();
     unsigned long long wbase = 0, tot = 0;
+    uint32_t lbase = 0, ltot = 0;
 #pragma unroll
     for (int k = 0; k < kWarps; ++k) {
-      unsigned long long v = wsum[k];
-      if (k < w) wbase += v;
+      const unsigned long long v = wsum[k];
+      const uint32_t lv = wlong[k];
+      if (k < w) {
+        wbase += v;
+        lbase += lv;
+      }
       tot += v;
+      ltot += lv;
     }
     unsigned long long excl = carry + wbase + incl - s;
+    uint32_t lexcl = lcarry + lbase + lincl - ls;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
       uint32_t p = t0 + threadIdx.x * kScanItems + k;
       if (p < end) offsets[p] = excl;
       excl += c[k];
+      if (long_list && (lmask >> k & 1u)) long_list[lexcl++] = p;
     }
     carry += tot;
+    lcarry += ltot;
     __syncthreads();
   }
 }
@@ -307,11 +366,15 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
 int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
                          unsigned long long* offsets, uint32_t* n_clamped,
                          unsigned long long* raw_total, uint32_t cap, uint32_t* status,
-                         ScanScratch& scratch, cudaStream_t s) {
-  scan_partial_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials);
-  scan_partials_kernel<<<1, kThreads, 0, s>>>(scratch.partials, cap, n_clamped, raw_total,
-                                              status);
-  scan_final_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, offsets);
+                         ScanScratch& scratch, cudaStream_t s, uint32_t* long_list,
+                         uint32_t* n_long) {
+  if (long_list && (!scratch.long_partials || !n_long)) return DS_ERR_ARG;
+  uint32_t* lp = long_list ? scratch.long_partials : nullptr;
+  scan_partial_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, lp);
+  scan_partials_kernel<<<1, kThreads, 0, s>>>(scratch.partials, lp, cap, n_clamped, raw_total,
+                                              long_list ? n_long : nullptr, status);
+  scan_final_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, offsets,
+                                                     lp, long_list);
   return cuda_status(cudaGetLastError());
 }
 
