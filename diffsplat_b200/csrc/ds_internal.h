@@ -41,7 +41,7 @@ constexpr int kSortBlocks = 296;    // 2 x 148 SMs
 constexpr int kSortTileItems = 2048;  // items per CTA iteration (8 warps x 32 lanes x 8)
 
 struct SortScratch {
-  uint32_t* hist = nullptr;  // [256 * kSortBlocks]
+  uint32_t* hist = nullptr;  // [256 * kSortBlocks] counts, then [256] digit totals
 };
 
 // Sorts n = min(*n_dev, cap) pairs by key bits [0, bits).  Pass 0 reads

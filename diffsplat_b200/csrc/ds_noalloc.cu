@@ -42,7 +42,7 @@ constexpr size_t kIsectBytes = 4 * (size_t)kMaxIsects;  // each of 6 pair arrays
 constexpr size_t kTotalBytes =
     13 * up256(16 * (size_t)kMaxSplats) +
     6 * up256(kIsectBytes) + 2 * up256(4 * (size_t)kMaxPixels) + up256(8 * (size_t)kMaxTiles) +
-    up256(4 * 256 * (size_t)kSortBlocks) + up256(8 * ((size_t)kSortBlocks + 1)) +
+    up256(4 * 256 * ((size_t)kSortBlocks + 1)) + up256(8 * ((size_t)kSortBlocks + 1)) +
     up256(sizeof(DevScalars));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kTotalBytes];
@@ -125,7 +125,7 @@ extern "C" int ds_raster_forward_noalloc(const ds_splat2d* in, int width, int he
   rb.alphas = c.take<float>(4 * (size_t)kMaxPixels);
   rb.last_ids = c.take<int32_t>(4 * (size_t)kMaxPixels);
   rb.ranges = c.take<int2>(8 * (size_t)kMaxTiles);
-  rb.sort.hist = c.take<uint32_t>(4 * 256 * (size_t)kSortBlocks);
+  rb.sort.hist = c.take<uint32_t>(4 * 256 * ((size_t)kSortBlocks + 1));
   rb.scan.partials = c.take<unsigned long long>(8 * ((size_t)kSortBlocks + 1));
   rb.scalars = c.take<DevScalars>(sizeof(DevScalars));
   // The forward does not produce gradients; these stay unset.

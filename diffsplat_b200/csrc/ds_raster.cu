@@ -204,21 +204,16 @@ int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStre
 
 __global__ void __launch_bounds__(kThreads)
     ranges_kernel(const uint32_t* __restrict__ sorted_tile, const uint32_t* __restrict__ n_dev,
-                  int tiles, int2* __restrict__ ranges) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= tiles) return;
+                  int* __restrict__ ranges) {
+  // ranges[t] = [first, last + 1) of tile t in the sorted pairs, from the
+  // boundaries between neighbouring ids (grid-stride; the ranges of tiles with
+  // no pair stay (0, 0) from the memset before).
   const uint32_t n = *n_dev;
-  auto lower = [&](uint32_t key) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi) >> 1;
-      if (sorted_tile[mid] < key) lo = mid + 1;
-      else hi = mid;
-    }
-    return lo;
-  };
-  uint32_t a = lower((uint32_t)t), b = lower((uint32_t)t + 1u);
-  ranges[t] = a < b ? make_int2((int)a, (int)b) : make_int2(0, 0);
+  for (uint32_t q = blockIdx.x * kThreads + threadIdx.x; q < n; q += gridDim.x * kThreads) {
+    const uint32_t t = sorted_tile[q];
+    if (q == 0 || sorted_tile[q - 1] != t) ranges[2 * (size_t)t] = (int)q;
+    if (q + 1 == n || sorted_tile[q + 1] != t) ranges[2 * (size_t)t + 1] = (int)(q + 1);
+  }
 }
 
 // Longest-first schedule of the composite CTAs: tiles bucketed by their list
@@ -337,7 +332,7 @@ static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   DS_TRY(alloc(&rb.emit_splat, c));
   DS_TRY(alloc(&rb.sorted_splat, c));
   DS_TRY(alloc(&rb.isect_grad, c * 9));
-  DS_TRY(alloc(&rb.sort.hist, (size_t)256 * kSortBlocks));
+  DS_TRY(alloc(&rb.sort.hist, (size_t)256 * (kSortBlocks + 1)));
   DS_TRY(alloc(&rb.scan.partials, (size_t)kSortBlocks + 1));
   DS_TRY(alloc(&rb.scan.long_partials, (size_t)kSortBlocks));
   DS_TRY(alloc(&rb.scalars, 1));
@@ -477,8 +472,13 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     }
   }
   // 5) per-tile ranges
-  ranges_kernel<<<(rb.tiles + kThreads - 1) / kThreads, kThreads, 0, s>>>(
-      rb.sorted_tile, &sc->n_isects, rb.tiles, rb.ranges);
+  DS_CUDA(cudaMemsetAsync(rb.ranges, 0, (size_t)rb.tiles * sizeof(int2), s));
+  {
+    const int64_t want = (rb.cap + kThreads - 1) / kThreads;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
+    ranges_kernel<<<blocks, kThreads, 0, s>>>(rb.sorted_tile, &sc->n_isects,
+                                              reinterpret_cast<int*>(rb.ranges));
+  }
   DS_CUDA(cudaGetLastError());
   if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST) {
     tile_order_kernel<<<1, 1024, 0, s>>>(rb.ranges, rb.tiles, rb.tile_order);

@@ -55,57 +55,37 @@ __global__ void __launch_bounds__(kThreads)
   hist[threadIdx.x * G + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of the digit-major histogram hist[digit * G + cta] with one
-// CTA of 1024 threads: warp w scans the G counts of digits w, w+32, ... in
-// coalesced 32-wide steps, then the 256 digit totals are scanned and added.
-__global__ void __launch_bounds__(1024) scan_hist_kernel(uint32_t* __restrict__ hist, int G) {
-  __shared__ uint32_t tot[256];
-  __shared__ uint32_t base[256];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int d = w; d < 256; d += 32) {
-    uint32_t* row = hist + (size_t)d * G;
-    uint32_t carry = 0;
-    for (int b0 = 0; b0 < G; b0 += 32) {
-      const int b = b0 + lane;
-      const uint32_t v = b < G ? row[b] : 0u;
-      uint32_t incl = v;
+// Row scan of the digit-major histogram hist[digit * G + cta]: one warp per
+// digit (256 / kWarps CTAs) loads its G counts at once, writes their exclusive
+// scan in place and the row total to hist[256 * kSortBlocks + digit].  The
+// scatter CTAs add the exclusive scan of the 256 totals themselves, so no
+// single CTA walks the whole histogram.
+constexpr int kRowChunks = (kSortBlocks + 31) / 32;
+
+__global__ void __launch_bounds__(kThreads) scan_hist_kernel(uint32_t* __restrict__ hist, int G) {
+  const int lane = threadIdx.x & 31;
+  const int d = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  uint32_t* row = hist + (size_t)d * G;
+  uint32_t v[kRowChunks];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (b < G) row[b] = carry + incl - v;
-      carry += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) tot[d] = carry;
+  for (int j = 0; j < kRowChunks; ++j) {
+    const int b = j * 32 + lane;
+    v[j] = b < G ? row[b] : 0u;
   }
-  __syncthreads();
-  if (w == 0) {
-    uint32_t v[8], s = 0;
+  uint32_t carry = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      v[k] = tot[lane * 8 + k];
-      s += v[k];
-    }
-    uint32_t incl = s;
+  for (int j = 0; j < kRowChunks; ++j) {
+    const int b = j * 32 + lane;
+    uint32_t incl = v[j];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += t;
     }
-    uint32_t run = incl - s;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      base[lane * 8 + k] = run;
-      run += v[k];
-    }
+    if (b < G) row[b] = carry + incl - v[j];
+    carry += __shfl_sync(0xffffffffu, incl, 31);
   }
-  __syncthreads();
-  for (int d = w; d < 256; d += 32) {
-    uint32_t* row = hist + (size_t)d * G;
-    const uint32_t add = base[d];
-    for (int b = lane; b < G; b += 32) row[b] += add;
-  }
+  if (lane == 0) hist[(size_t)256 * kSortBlocks + d] = carry;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -122,7 +102,23 @@ __global__ void __launch_bounds__(kThreads)
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
-  base[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x];
+  {
+    // digit base = exclusive scan of the digit totals + this CTA's row offset
+    __shared__ uint32_t wt[kWarps];
+    const uint32_t tv = offs[(size_t)256 * kSortBlocks + threadIdx.x];
+    uint32_t incl = tv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wt[w] = incl;
+    __syncthreads();
+    uint32_t wb = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) wb += k < w ? wt[k] : 0u;
+    base[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x] + wb + incl - tv;
+  }
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t t0 = begin; t0 < end; t0 += kSortTileItems) {
     for (int d = lane; d < 256; d += 32) cnt[w][d] = 0;
@@ -349,7 +345,7 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
     const int shift = 8 * p;
     const bool last = p == passes - 1;
     radix_hist_kernel<<<G, kThreads, 0, s>>>(src_k, n_dev, cap, shift, scratch.hist);
-    scan_hist_kernel<<<1, 1024, 0, s>>>(scratch.hist, G);
+    scan_hist_kernel<<<256 / kWarps, kThreads, 0, s>>>(scratch.hist, G);
     radix_scatter_kernel<<<G, kThreads, 0, s>>>(
         src_k, src_v, src_v == nullptr ? 1 : 0, dst_k, dst_v, n_dev, cap, shift, scratch.hist,
         last ? gather_src : nullptr, last ? gather_dst : nullptr);
