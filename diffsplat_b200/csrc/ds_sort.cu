@@ -44,12 +44,20 @@ __global__ void __launch_bounds__(kThreads)
   h[threadIdx.x] = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  // Warp-aggregated shared-memory counting: one atomic per distinct digit per warp.
-  for (uint32_t base = begin; base < end; base += kThreads) {
-    uint32_t i = base + threadIdx.x;
-    uint32_t d = i < end ? ((keys[i] >> shift) & 255u) : 0x100u;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  // kItems loads in flight per thread, then warp-aggregated shared-memory
+  // counting: one atomic per distinct digit per warp and item slot.
+  for (uint32_t t0 = begin; t0 < end; t0 += kSortTileItems) {
+    uint32_t d[kItems];
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const uint32_t i = t0 + it * kThreads + threadIdx.x;
+      d[it] = i < end ? ((keys[i] >> shift) & 255u) : 0x100u;
+    }
+#pragma unroll
+    for (int it = 0; it < kItems; ++it) {
+      const uint32_t peers = __match_any_sync(0xffffffffu, d[it]);
+      if (d[it] < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d[it]], (uint32_t)__popc(peers));
+    }
   }
   __syncthreads();
   hist[threadIdx.x * G + blockIdx.x] = h[threadIdx.x];
@@ -88,25 +96,31 @@ __global__ void __launch_bounds__(kThreads) scan_hist_kernel(uint32_t* __restric
   if (lane == 0) hist[(size_t)256 * kSortBlocks + d] = carry;
 }
 
+// Each CTA takes its chunk 2048 items at a time: ranks them stably inside each
+// warp with __match_any_sync, turns the per-warp digit counts into tile-local
+// offsets, stages the tile in digit order in shared memory and writes it out
+// in that order, so items of one digit leave as contiguous runs.
 __global__ void __launch_bounds__(kThreads)
     radix_scatter_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                          int iota, uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                          const uint32_t* __restrict__ n_dev, uint32_t cap, int shift,
                          const uint32_t* __restrict__ offs, const uint32_t* __restrict__ gsrc,
                          uint32_t* __restrict__ gdst) {
-  __shared__ uint32_t cnt[kWarps][256];
-  __shared__ uint32_t base[256];
+  __shared__ uint32_t cnt[kWarps][256];  // per-warp digit counts, then per-warp offsets
+  __shared__ uint32_t gbase[256];        // output position of the tile's first item of a digit
+  __shared__ uint32_t lstart[256];       // tile-local start of each digit
+  __shared__ uint32_t skey[kSortTileItems];
+  __shared__ uint32_t sval[kSortTileItems];
+  __shared__ uint32_t wt[kWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t n = min(*n_dev, cap);
   const uint32_t chunk = sort_chunk(n, gridDim.x);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
-  {
-    // digit base = exclusive scan of the digit totals + this CTA's row offset
-    __shared__ uint32_t wt[kWarps];
-    const uint32_t tv = offs[(size_t)256 * kSortBlocks + threadIdx.x];
-    uint32_t incl = tv;
+  // thread t owns digit t: block exclusive scan of a per-digit value
+  auto block_excl = [&](uint32_t v) {
+    uint32_t incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -117,8 +131,12 @@ __global__ void __launch_bounds__(kThreads)
     uint32_t wb = 0;
 #pragma unroll
     for (int k = 0; k < kWarps; ++k) wb += k < w ? wt[k] : 0u;
-    base[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x] + wb + incl - tv;
-  }
+    __syncthreads();
+    return wb + incl - v;
+  };
+  // digit base = exclusive scan of the digit totals + this CTA's row offset
+  gbase[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x] +
+                       block_excl(offs[(size_t)256 * kSortBlocks + threadIdx.x]);
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t t0 = begin; t0 < end; t0 += kSortTileItems) {
     for (int d = lane; d < 256; d += 32) cnt[w][d] = 0;
@@ -126,46 +144,59 @@ __global__ void __launch_bounds__(kThreads)
     uint32_t key[kItems], val[kItems], rank[kItems];
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-      uint32_t idx = t0 + w * 256 + it * 32 + lane;
-      bool ok = idx < end;
+      const uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      const bool ok = idx < end;
       key[it] = ok ? kin[idx] : 0u;
       val[it] = ok ? (iota ? idx : vin[idx]) : 0u;
     }
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-      uint32_t idx = t0 + w * 256 + it * 32 + lane;
-      bool ok = idx < end;
-      uint32_t d = ok ? ((key[it] >> shift) & 255u) : 0x100u;
-      uint32_t peers = __match_any_sync(0xffffffffu, d);
-      uint32_t pre = ok ? cnt[w][d] : 0u;
+      const uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      const bool ok = idx < end;
+      const uint32_t d = ok ? ((key[it] >> shift) & 255u) : 0x100u;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t pre = ok ? cnt[w][d] : 0u;
       __syncwarp();
       if (ok && lane == __ffs(peers) - 1) cnt[w][d] = pre + __popc(peers);
       __syncwarp();
       rank[it] = pre + __popc(peers & lt);
     }
     __syncthreads();
+    uint32_t total;
     {
-      uint32_t run = base[threadIdx.x];
+      uint32_t run = 0;
 #pragma unroll
       for (int ww = 0; ww < kWarps; ++ww) {
-        uint32_t c = cnt[ww][threadIdx.x];
+        const uint32_t c = cnt[ww][threadIdx.x];
         cnt[ww][threadIdx.x] = run;
         run += c;
       }
-      base[threadIdx.x] = run;
+      total = run;
+      lstart[threadIdx.x] = block_excl(run);
     }
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-      uint32_t idx = t0 + w * 256 + it * 32 + lane;
+      const uint32_t idx = t0 + w * 256 + it * 32 + lane;
       if (idx < end) {
-        uint32_t d = (key[it] >> shift) & 255u;
-        uint32_t dst = cnt[w][d] + rank[it];
-        kout[dst] = key[it];
-        vout[dst] = val[it];
-        if (gdst) gdst[dst] = gsrc[val[it]];
+        const uint32_t d = (key[it] >> shift) & 255u;
+        const uint32_t lp = lstart[d] + cnt[w][d] + rank[it];
+        skey[lp] = key[it];
+        sval[lp] = val[it];
       }
     }
+    __syncthreads();
+    const uint32_t items = min(end - t0, (uint32_t)kSortTileItems);
+    for (uint32_t j = threadIdx.x; j < items; j += kThreads) {
+      const uint32_t k = skey[j], v = sval[j];
+      const uint32_t d = (k >> shift) & 255u;
+      const uint32_t dst = gbase[d] + j - lstart[d];
+      kout[dst] = k;
+      vout[dst] = v;
+      if (gdst) gdst[dst] = gsrc[v];
+    }
+    __syncthreads();
+    gbase[threadIdx.x] += total;
     __syncthreads();
   }
 }
