@@ -31,8 +31,16 @@ namespace ds {
 namespace {
 
 constexpr int kFwdBatch = 256;  // splats staged in shared memory per forward batch
+#ifndef DS_FWD_GROUP
+#define DS_FWD_GROUP 4
+#endif
+constexpr int kFwdGroup = DS_FWD_GROUP;  // forward hits evaluated together
+#ifndef DS_BWD_GROUP
+#define DS_BWD_GROUP 2
+#endif
+constexpr int kBwdGroup = DS_BWD_GROUP;  // backward hits evaluated together
 #ifndef DS_FWD_MIN_BLOCKS
-#define DS_FWD_MIN_BLOCKS 5
+#define DS_FWD_MIN_BLOCKS 4
 #endif
 #ifndef DS_BWD_MIN_BLOCKS
 #define DS_BWD_MIN_BLOCKS 4
@@ -150,6 +158,15 @@ __device__ __forceinline__ bool ellipse_hits(const float4& a, const float4& b, f
   return 0.5f * m <= cut;
 }
 
+// Forward alpha of a splat at a pixel (0 when the splat is skipped there):
+// sigma < 0 or beyond the cut, or alpha below 1/255.
+__device__ __forceinline__ float splat_alpha(float dx, float dy, const float4& b, float cut) {
+  const float sigma = 0.5f * conic_dist2(dx, dy, b.x, b.y, b.z);
+  if (sigma < 0.f || sigma > cut) return 0.f;
+  const float alpha = fminf(kMaxAlpha, b.w * __expf(-sigma));
+  return alpha < kAlphaThres ? 0.f : alpha;
+}
+
 // One splat of a batch, loaded into registers a batch ahead of its use so the
 // gathers overlap the current batch's compositing.
 struct Staged {
@@ -248,30 +265,47 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     for (int kw = 0; kw * 32 < bs && !stop; ++kw) {
       const int l = kw * 32 + lane;
       uint32_t word = __ballot_sync(0xffffffffu, l < bs && ((sMask[l] >> w) & 1u));
+      // Hits are taken kFwdGroup at a time: all their alphas are computed
+      // before any is composited (front to back), so the conic / exp chains of
+      // the group overlap.
       while (word) {
-        const int t = kw * 32 + __ffs(word) - 1;
-        word &= word - 1u;
-        const float4 a = sA[t];
-        const float4 b = sB[t];
-        const float4 c = sC[t];
-        const float dx = a.x - m.px;
+        int tg[kFwdGroup];
+        int ng = 0;
+#pragma unroll
+        for (int g = 0; g < kFwdGroup; ++g) {
+          tg[g] = word ? kw * 32 + __ffs(word) - 1 : tg[0];  // word is warp-uniform
+          ng += word ? 1 : 0;
+          word &= word - 1u;
+        }
+        float4 ag[kFwdGroup], bg[kFwdGroup], cg[kFwdGroup];
+#pragma unroll
+        for (int g = 0; g < kFwdGroup; ++g) {
+          ag[g] = sA[tg[g]];
+          bg[g] = sB[tg[g]];
+          cg[g] = sC[tg[g]];
+        }
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
           if (done[k]) continue;
-          if (kCount) ++n_tested;
-          const float dy = a.y - m.py[k];
-          const float sigma = 0.5f * conic_dist2(dx, dy, b.x, b.y, b.z);
-          if (sigma < 0.f || sigma > c.w) continue;
-          const float alpha = fminf(kMaxAlpha, b.w * __expf(-sigma));
-          if (alpha < kAlphaThres) continue;
-          if (kCount) ++n_contrib;
-          const float vis = alpha * T[k];
-          Cr[k] = __fmaf_rn(c.x, vis, Cr[k]);
-          Cg[k] = __fmaf_rn(c.y, vis, Cg[k]);
-          Cb[k] = __fmaf_rn(c.z, vis, Cb[k]);
-          cur[k] = (uint32_t)(b0 + t);
-          T[k] = T[k] * (1.f - alpha);
-          if (T[k] <= kTThres) done[k] = true;
+          float al[kFwdGroup];
+#pragma unroll
+          for (int g = 0; g < kFwdGroup; ++g)
+            al[g] = splat_alpha(ag[g].x - m.px, ag[g].y - m.py[k], bg[g], cg[g].w);
+#pragma unroll
+          for (int g = 0; g < kFwdGroup; ++g) {
+            if (g >= ng || done[k]) break;
+            if (kCount) ++n_tested;
+            if (al[g] > 0.f) {
+              if (kCount) ++n_contrib;
+              const float vis = al[g] * T[k];
+              Cr[k] = __fmaf_rn(cg[g].x, vis, Cr[k]);
+              Cg[k] = __fmaf_rn(cg[g].y, vis, Cg[k]);
+              Cb[k] = __fmaf_rn(cg[g].z, vis, Cb[k]);
+              cur[k] = (uint32_t)(b0 + tg[g]);
+              T[k] = T[k] * (1.f - al[g]);
+              if (T[k] <= kTThres) done[k] = true;
+            }
+          }
         }
         all_done = true;
 #pragma unroll
@@ -453,64 +487,97 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
       const int l = kw * 32 + lane;
       uint32_t word =
           __ballot_sync(0xffffffffu, l >= t_start && l < bs && ((sMask[l] >> w) & 1u));
+      // Hits are taken kBwdGroup at a time: the conic / exp / alpha of all of
+      // them first (independent of T), then the recurrence back to front, then
+      // the warp reductions, which overlap.
       while (word) {
-        const int t = kw * 32 + __ffs(word) - 1;
-        word &= word - 1u;
-        const float4 a = sA[t];
-        const float4 b = sB[t];
-        const float4 c = sC[t];
-        const float idet = sI[t];
-        const float dx = a.x - m.px;
-        const int sidx = batch_end - t;
-        float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float va = 0.f;
-        bool any = false;
+        int tg[kBwdGroup];
+        int ng = 0;
+#pragma unroll
+        for (int g = 0; g < kBwdGroup; ++g) {
+          tg[g] = word ? kw * 32 + __ffs(word) - 1 : tg[0];  // word is warp-uniform
+          ng += word ? 1 : 0;
+          word &= word - 1u;
+        }
+        float4 ag[kBwdGroup], bg[kBwdGroup], cg[kBwdGroup];
+        float ig[kBwdGroup];
+#pragma unroll
+        for (int g = 0; g < kBwdGroup; ++g) {
+          ag[g] = sA[tg[g]];
+          bg[g] = sB[tg[g]];
+          cg[g] = sC[tg[g]];
+          ig[g] = sI[tg[g]];
+        }
+        float v[kBwdGroup][8], va[kBwdGroup];
+        bool any[kBwdGroup];
+#pragma unroll
+        for (int g = 0; g < kBwdGroup; ++g) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) v[g][q] = 0.f;
+          va[g] = 0.f;
+          any[g] = false;
+        }
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-          if (!(m.inside[k] && sidx <= fin[k])) continue;
-          const float dy = a.y - m.py[k];
-          const float dist2 = conic_dist2(dx, dy, b.x, b.y, b.z);
-          const float sigma = 0.5f * dist2;
-          if (sigma < 0.f || sigma > c.w) continue;
-          const float opac = b.w;
-          const float g_exp = __expf(-sigma);
-          const float alpha = fminf(kMaxAlpha, opac * g_exp);
-          if (alpha < kAlphaThres) continue;
-          any = true;
-          const float T_before = T[k] / fmaxf(1.f - alpha, 1e-6f);
-          const float fac = alpha * T_before;
-          v[0] += fac * gr[k];
-          v[1] += fac * gg[k];
-          v[2] += fac * gb[k];
-          // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
-          // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
-          // exact derivative divides it by T_after instead.
-          const float ia = kExact ? 1.f / T[k] : 1.f;
-          const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
-                                            (c.y - accg[k] * ia) * gg[k] +
-                                            (c.z - accb[k] * ia) * gb[k]);
-          if (opac * g_exp <= kMaxAlpha) {
-            va += g_exp * v_alpha;
-            const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
-            const float ddx = 2.f * (dx * b.x + dy * b.y);
-            const float ddy = 2.f * (dx * b.y + dy * b.z);
-            v[3] += v_dist2 * ddx;
-            v[4] += v_dist2 * ddy;
-            v[5] += v_dist2 * (-0.25f * ddx * ddx);
-            v[7] += v_dist2 * (-0.25f * ddy * ddy);
-            v[6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * idet);
+          if (!m.inside[k]) continue;
+          float dxg[kBwdGroup], dyg[kBwdGroup], d2g[kBwdGroup], eg[kBwdGroup], alg[kBwdGroup];
+          bool pg[kBwdGroup];
+#pragma unroll
+          for (int g = 0; g < kBwdGroup; ++g) {
+            dxg[g] = ag[g].x - m.px;
+            dyg[g] = ag[g].y - m.py[k];
+            d2g[g] = conic_dist2(dxg[g], dyg[g], bg[g].x, bg[g].y, bg[g].z);
+            const float sigma = 0.5f * d2g[g];
+            eg[g] = __expf(-sigma);
+            alg[g] = fminf(kMaxAlpha, bg[g].w * eg[g]);
+            pg[g] = g < ng && batch_end - tg[g] <= fin[k] && !(sigma < 0.f || sigma > cg[g].w) &&
+                    !(alg[g] < kAlphaThres);
           }
-          accr[k] += c.x * fac;
-          accg[k] += c.y * fac;
-          accb[k] += c.z * fac;
-          T[k] = T_before;
+#pragma unroll
+          for (int g = 0; g < kBwdGroup; ++g) {
+            if (!pg[g]) continue;
+            const float4 b = bg[g], c = cg[g];
+            const float dx = dxg[g], dy = dyg[g], dist2 = d2g[g], g_exp = eg[g], alpha = alg[g];
+            const float opac = b.w;
+            any[g] = true;
+            const float T_before = T[k] / fmaxf(1.f - alpha, 1e-6f);
+            const float fac = alpha * T_before;
+            v[g][0] += fac * gr[k];
+            v[g][1] += fac * gg[k];
+            v[g][2] += fac * gb[k];
+            // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
+            // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
+            // exact derivative divides it by T_after instead.
+            const float ia = kExact ? 1.f / T[k] : 1.f;
+            const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
+                                              (c.y - accg[k] * ia) * gg[k] +
+                                              (c.z - accb[k] * ia) * gb[k]);
+            if (opac * g_exp <= kMaxAlpha) {
+              va[g] += g_exp * v_alpha;
+              const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
+              const float ddx = 2.f * (dx * b.x + dy * b.y);
+              const float ddy = 2.f * (dx * b.y + dy * b.z);
+              v[g][3] += v_dist2 * ddx;
+              v[g][4] += v_dist2 * ddy;
+              v[g][5] += v_dist2 * (-0.25f * ddx * ddx);
+              v[g][7] += v_dist2 * (-0.25f * ddy * ddy);
+              v[g][6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * ig[g]);
+            }
+            accr[k] += c.x * fac;
+            accg[k] += c.y * fac;
+            accb[k] += c.z * fac;
+            T[k] = T_before;
+          }
         }
-        if (!__any_sync(0xffffffffu, any)) continue;
-        // lane 4q ends up with the warp sum of v[q]
-        const float s8 = warp_sum8_transposed(v, lane);
-        const float sa = warp_sum(va);
-        if ((lane & 3) == 0) part[w][t * 9 + (lane >> 2)] = s8;
-        if (lane == 0) part[w][t * 9 + 8] = sa;
+#pragma unroll
+        for (int g = 0; g < kBwdGroup; ++g) {
+          if (!__any_sync(0xffffffffu, any[g])) continue;
+          // lane 4q ends up with the warp sum of v[q]
+          const float s8 = warp_sum8_transposed(v[g], lane);
+          const float sa = warp_sum(va[g]);
+          if ((lane & 3) == 0) part[w][tg[g] * 9 + (lane >> 2)] = s8;
+          if (lane == 0) part[w][tg[g] * 9 + 8] = sa;
+        }
       }
     }
     __syncthreads();
