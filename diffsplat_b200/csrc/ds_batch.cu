@@ -70,6 +70,7 @@ struct ds_batch {
   uint16_t* tile_inst = nullptr;
   ds::InstGeom* geom_dev = nullptr;
   ds::Camera* cams = nullptr;
+  ds::HostStage cam_stage;
   ds::RasterBuffers rb;
   float2* bc_table = nullptr;
   float2* bc_cur = nullptr;
@@ -332,8 +333,7 @@ int ds_batch_set_camera(ds_batch* b, int k, const float pv[16], const float cam_
   for (int q = 0; q < 16; ++q) c.pv[q] = pv[q];
   for (int q = 0; q < 3; ++q) c.cam[q] = cam_pos[q];
   c.pad = 0.f;
-  DS_CUDA(cudaMemcpyAsync(b->cams + k, &c, sizeof(c), cudaMemcpyHostToDevice,
-                          (cudaStream_t)stream));
+  DS_TRY(b->cam_stage.upload(b->cams + k, &c, sizeof(c), (cudaStream_t)stream));
   return DS_OK;
 }
 

@@ -50,6 +50,7 @@ struct ds_fitter {
   float* image = nullptr;
   ds::RasterBuffers rb;
   ds::Camera* cam_dev = nullptr;
+  ds::HostStage cam_stage;
   float2* bc_table = nullptr;
   float2* bc_cur = nullptr;
   int bc_len = 0;
@@ -279,9 +280,7 @@ int ds_fitter_set_camera(ds_fitter* f, const float pv[16], const float cam_pos[3
   for (int k = 0; k < 16; ++k) c.pv[k] = pv[k];
   for (int k = 0; k < 3; ++k) c.cam[k] = cam_pos[k];
   c.pad = 0.f;
-  DS_CUDA(cudaMemcpyAsync(f->cam_dev, &c, sizeof(c), cudaMemcpyHostToDevice, (cudaStream_t)stream));
-  // cudaMemcpyAsync from pageable memory returns after staging the source, so
-  // the local may go out of scope.
+  DS_TRY(f->cam_stage.upload(f->cam_dev, &c, sizeof(c), (cudaStream_t)stream));
   f->have_camera = true;
   return DS_OK;
 }

@@ -21,6 +21,25 @@ inline int cuda_status(cudaError_t e) {
 
 #define DS_CUDA(expr) DS_TRY(::ds::cuda_status(expr))
 
+// Small host -> device uploads (cameras) through a ring of pinned slots
+// (ds_stage.cu): an upload waits only for the copy that used its slot kSlots
+// uploads earlier, never for the stream, and no pending copy sees its source
+// change.  A copy from pageable memory would instead return only once the
+// stream had reached it.
+struct HostStage {
+  static constexpr int kSlots = 8;
+  static constexpr size_t kSlotBytes = 128;
+  unsigned char* host = nullptr;
+  cudaEvent_t ev[kSlots] = {};
+  int next = 0;
+  HostStage() = default;
+  HostStage(const HostStage&) = delete;
+  HostStage& operator=(const HostStage&) = delete;
+  ~HostStage();
+  int upload(void* dst, const void* src, size_t bytes, cudaStream_t s);
+  void release();
+};
+
 // Layer kernels (ds_activ_project.cu)
 int launch_activ_forward(const ds_gaussian3d& in, int degree, const float cam[3],
                          const ds_splat3d& out, cudaStream_t s);

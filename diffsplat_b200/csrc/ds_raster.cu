@@ -69,33 +69,82 @@ __global__ void __launch_bounds__(kThreads)
                 int n, int ntx, uint32_t cap, uint32_t* __restrict__ tile_keys,
                 uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start,
                 const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom) {
-  // One warp per splat in depth order; lanes write its tiles (row-major over
-  // the rectangle) to consecutive emission slots.  In a batch the tile id is
+  // Four lanes (a quad) per splat in depth order: they load its count, offset
+  // and tile rectangle and write its tiles (row-major over the rectangle) to
+  // consecutive emission slots, four at a time.  Splats with more than
+  // kQuadTiles tiles are written by the whole warp instead, one after another,
+  // their values broadcast from the quad.  In a batch the tile id is
   // batch-wide: the instance's first tile plus its row-major tile index.
-  const int p = (int)((blockIdx.x * (unsigned)kThreads + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (p >= n) return;
-  const uint32_t i = perm[p];
-  const uint32_t c = counts[i];
-  if (c == 0) return;
-  const unsigned long long off = offsets[p];
-  if (lane == 0) seg_start[i] = (uint32_t)(off < cap ? off : cap);
-  if (off >= cap) return;
-  const ushort4 r = rect[i];
-  const uint32_t w = (uint32_t)(r.y - r.x + 1);
-  unsigned long long end = off + c;
-  if (end > cap) end = cap;
-  const uint32_t m = (uint32_t)(end - off);
-  uint32_t base = 0, pitch = (uint32_t)ntx;
-  if (geom) {
-    const InstGeom g = geom[inst_of_splat[i]];
-    base = (uint32_t)g.tile_off;
-    pitch = (uint32_t)g.ntx;
+  constexpr uint32_t kQuadTiles = 64;
+  const int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31, q = lane & 3;
+  if ((t - lane) / 4 >= n) return;  // uniform per warp
+  const int p = (int)(t / 4);
+  uint32_t i = 0, m = 0, x0 = 0, w = 1, y0 = 0, base = 0, pitch = (uint32_t)ntx;
+  unsigned long long off = 0;
+  if (p < n) {
+    i = perm[p];
+    const uint32_t c = counts[i];
+    if (c) {
+      off = offsets[p];
+      if (q == 0) seg_start[i] = (uint32_t)(off < cap ? off : cap);
+      if (off < cap) {
+        unsigned long long end = off + c;
+        if (end > cap) end = cap;
+        m = (uint32_t)(end - off);
+        const ushort4 r = rect[i];
+        x0 = r.x;
+        w = (uint32_t)(r.y - r.x + 1);
+        y0 = r.z;
+        if (geom) {
+          const InstGeom g = geom[inst_of_splat[i]];
+          base = (uint32_t)g.tile_off;
+          pitch = (uint32_t)g.ntx;
+        }
+      }
+    }
   }
-  for (uint32_t k = lane; k < m; k += 32) {
-    const uint32_t ty = r.z + k / w, tx = r.x + k % w;
-    tile_keys[off + k] = base + ty * pitch + tx;
-    emit_splat[off + k] = i;
+  // Row of entry k of a rectangle wd tiles wide: a float estimate from the
+  // reciprocal (off by at most a few for k < 2^24), stepped to the exact
+  // floor(k / wd).
+  auto row_of = [](uint32_t k, uint32_t wd, float inv) {
+    uint32_t r = (uint32_t)((float)k * inv);
+    while (r > 0u && r * wd > k) --r;
+    while ((r + 1u) * wd <= k) ++r;
+    return r;
+  };
+  if (m > 0 && m <= kQuadTiles) {
+    const float inv = 1.f / (float)w;
+    const uint32_t row0 = base + y0 * pitch + x0;
+    for (uint32_t k = q; k < m; k += 4) {
+      const uint32_t ty = row_of(k, w, inv);
+      tile_keys[off + k] = row0 + ty * pitch + (k - ty * w);
+      emit_splat[off + k] = i;
+    }
+  }
+  uint32_t todo = __ballot_sync(0xffffffffu, q == 0 && m > kQuadTiles);
+  const bool batch = geom != nullptr;  // uniform
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1u;
+    const uint32_t sm = __shfl_sync(0xffffffffu, m, src);
+    const uint32_t soff = __shfl_sync(0xffffffffu, (uint32_t)off, src);  // off < cap < 2^32
+    const uint32_t si = __shfl_sync(0xffffffffu, i, src);
+    const uint32_t sx = __shfl_sync(0xffffffffu, x0, src);
+    const uint32_t sw = __shfl_sync(0xffffffffu, w, src);
+    const uint32_t sy = __shfl_sync(0xffffffffu, y0, src);
+    uint32_t sb = 0, sp = pitch;
+    if (batch) {
+      sb = __shfl_sync(0xffffffffu, base, src);
+      sp = __shfl_sync(0xffffffffu, pitch, src);
+    }
+    const float sinv = 1.f / (float)sw;
+    const uint32_t row0 = sb + sy * sp + sx;
+    for (uint32_t k = lane; k < sm; k += 32) {
+      const uint32_t ty = row_of(k, sw, sinv);
+      tile_keys[soff + k] = row0 + ty * sp + (k - ty * sw);
+      emit_splat[soff + k] = si;
+    }
   }
 }
 
@@ -452,7 +501,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
                                 &sc->n_isects, &sc->n_isects_raw, (uint32_t)rb.cap, &sc->status,
                                 rb.scan, s, with_long_list ? rb.long_list : nullptr, &sc->n_long));
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
-    emit_kernel<<<(unsigned)(((int64_t)n * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+    emit_kernel<<<(unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
         rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom);
     DS_CUDA(cudaGetLastError());

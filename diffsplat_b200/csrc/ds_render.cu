@@ -23,6 +23,7 @@ struct ds_renderer {
   ds::Soa<__nv_bfloat16> R16{};
   ds::RasterBuffers rb;
   ds::Camera* cam_dev = nullptr;
+  ds::HostStage cam_stage;
   float* image = nullptr;
   bool have_params = false;
 };
@@ -120,7 +121,7 @@ int ds_renderer_render(ds_renderer* r, const float pv[16], const float cam_pos[3
   for (int k = 0; k < 16; ++k) c.pv[k] = pv[k];
   for (int k = 0; k < 3; ++k) c.cam[k] = cam_pos[k];
   c.pad = 0.f;
-  DS_CUDA(cudaMemcpyAsync(r->cam_dev, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  DS_TRY(r->cam_stage.upload(r->cam_dev, &c, sizeof(c), s));
   ds::RasterBuffers& rb = r->rb;
   DS_CUDA(cudaMemsetAsync(&rb.scalars->visible, 0, sizeof(uint32_t), s));
   const int n = r->count;
