@@ -34,11 +34,11 @@ constexpr int kFwdBatch = 256;  // splats staged in shared memory per forward ba
 #ifndef DS_FWD_GROUP
 #define DS_FWD_GROUP 4
 #endif
-constexpr int kFwdGroup = DS_FWD_GROUP;  // forward hits evaluated together
+constexpr int kFwdGroupPpt1 = DS_FWD_GROUP;  // forward hits evaluated together at 1 px/thread
 #ifndef DS_BWD_GROUP
 #define DS_BWD_GROUP 2
 #endif
-constexpr int kBwdGroup = DS_BWD_GROUP;  // backward hits evaluated together
+constexpr int kBwdGroupPpt1 = DS_BWD_GROUP;  // backward hits evaluated together at 1 px/thread
 #ifndef DS_FWD_MIN_BLOCKS
 #define DS_FWD_MIN_BLOCKS 4
 #endif
@@ -59,6 +59,12 @@ struct Lay {
   // resident CTAs per SM the register allocation must allow (256-thread CTAs)
   static constexpr int kMinBlocksFwd = kThreads == 256 ? DS_FWD_MIN_BLOCKS : 1;
   static constexpr int kMinBlocksBwd = kThreads == 256 ? DS_BWD_MIN_BLOCKS : 1;
+  // hits evaluated together: only at 1 pixel per thread; with more pixels the
+  // per-pixel state already fills the registers (batch64, B200: grouping
+  // at 2 pixels per thread cost 0.6% there and 5% before the backward
+  // was limited to one hit per group)
+  static constexpr int kFwdGroup = PPT == 1 ? kFwdGroupPpt1 : 1;
+  static constexpr int kBwdGroup = PPT == 1 ? kBwdGroupPpt1 : 1;
   static_assert(kThreads % 32 == 0 && BW <= TS && kWarps <= 32, "unsupported tile layout");
 };
 
@@ -265,21 +271,21 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     for (int kw = 0; kw * 32 < bs && !stop; ++kw) {
       const int l = kw * 32 + lane;
       uint32_t word = __ballot_sync(0xffffffffu, l < bs && ((sMask[l] >> w) & 1u));
-      // Hits are taken kFwdGroup at a time: all their alphas are computed
+      // Hits are taken Lc::kFwdGroup at a time: all their alphas are computed
       // before any is composited (front to back), so the conic / exp chains of
       // the group overlap.
       while (word) {
-        int tg[kFwdGroup];
+        int tg[Lc::kFwdGroup];
         int ng = 0;
 #pragma unroll
-        for (int g = 0; g < kFwdGroup; ++g) {
+        for (int g = 0; g < Lc::kFwdGroup; ++g) {
           tg[g] = word ? kw * 32 + __ffs(word) - 1 : tg[0];  // word is warp-uniform
           ng += word ? 1 : 0;
           word &= word - 1u;
         }
-        float4 ag[kFwdGroup], bg[kFwdGroup], cg[kFwdGroup];
+        float4 ag[Lc::kFwdGroup], bg[Lc::kFwdGroup], cg[Lc::kFwdGroup];
 #pragma unroll
-        for (int g = 0; g < kFwdGroup; ++g) {
+        for (int g = 0; g < Lc::kFwdGroup; ++g) {
           ag[g] = sA[tg[g]];
           bg[g] = sB[tg[g]];
           cg[g] = sC[tg[g]];
@@ -287,12 +293,12 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
           if (done[k]) continue;
-          float al[kFwdGroup];
+          float al[Lc::kFwdGroup];
 #pragma unroll
-          for (int g = 0; g < kFwdGroup; ++g)
+          for (int g = 0; g < Lc::kFwdGroup; ++g)
             al[g] = splat_alpha(ag[g].x - m.px, ag[g].y - m.py[k], bg[g], cg[g].w);
 #pragma unroll
-          for (int g = 0; g < kFwdGroup; ++g) {
+          for (int g = 0; g < Lc::kFwdGroup; ++g) {
             if (g >= ng || done[k]) break;
             if (kCount) ++n_tested;
             if (al[g] > 0.f) {
@@ -487,31 +493,31 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
       const int l = kw * 32 + lane;
       uint32_t word =
           __ballot_sync(0xffffffffu, l >= t_start && l < bs && ((sMask[l] >> w) & 1u));
-      // Hits are taken kBwdGroup at a time: the conic / exp / alpha of all of
+      // Hits are taken Lc::kBwdGroup at a time: the conic / exp / alpha of all of
       // them first (independent of T), then the recurrence back to front, then
       // the warp reductions, which overlap.
       while (word) {
-        int tg[kBwdGroup];
+        int tg[Lc::kBwdGroup];
         int ng = 0;
 #pragma unroll
-        for (int g = 0; g < kBwdGroup; ++g) {
+        for (int g = 0; g < Lc::kBwdGroup; ++g) {
           tg[g] = word ? kw * 32 + __ffs(word) - 1 : tg[0];  // word is warp-uniform
           ng += word ? 1 : 0;
           word &= word - 1u;
         }
-        float4 ag[kBwdGroup], bg[kBwdGroup], cg[kBwdGroup];
-        float ig[kBwdGroup];
+        float4 ag[Lc::kBwdGroup], bg[Lc::kBwdGroup], cg[Lc::kBwdGroup];
+        float ig[Lc::kBwdGroup];
 #pragma unroll
-        for (int g = 0; g < kBwdGroup; ++g) {
+        for (int g = 0; g < Lc::kBwdGroup; ++g) {
           ag[g] = sA[tg[g]];
           bg[g] = sB[tg[g]];
           cg[g] = sC[tg[g]];
           ig[g] = sI[tg[g]];
         }
-        float v[kBwdGroup][8], va[kBwdGroup];
-        bool any[kBwdGroup];
+        float v[Lc::kBwdGroup][8], va[Lc::kBwdGroup];
+        bool any[Lc::kBwdGroup];
 #pragma unroll
-        for (int g = 0; g < kBwdGroup; ++g) {
+        for (int g = 0; g < Lc::kBwdGroup; ++g) {
 #pragma unroll
           for (int q = 0; q < 8; ++q) v[g][q] = 0.f;
           va[g] = 0.f;
@@ -520,10 +526,10 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
           if (!m.inside[k]) continue;
-          float dxg[kBwdGroup], dyg[kBwdGroup], d2g[kBwdGroup], eg[kBwdGroup], alg[kBwdGroup];
-          bool pg[kBwdGroup];
+          float dxg[Lc::kBwdGroup], dyg[Lc::kBwdGroup], d2g[Lc::kBwdGroup], eg[Lc::kBwdGroup], alg[Lc::kBwdGroup];
+          bool pg[Lc::kBwdGroup];
 #pragma unroll
-          for (int g = 0; g < kBwdGroup; ++g) {
+          for (int g = 0; g < Lc::kBwdGroup; ++g) {
             dxg[g] = ag[g].x - m.px;
             dyg[g] = ag[g].y - m.py[k];
             d2g[g] = conic_dist2(dxg[g], dyg[g], bg[g].x, bg[g].y, bg[g].z);
@@ -534,7 +540,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                     !(alg[g] < kAlphaThres);
           }
 #pragma unroll
-          for (int g = 0; g < kBwdGroup; ++g) {
+          for (int g = 0; g < Lc::kBwdGroup; ++g) {
             if (!pg[g]) continue;
             const float4 b = bg[g], c = cg[g];
             const float dx = dxg[g], dy = dyg[g], dist2 = d2g[g], g_exp = eg[g], alpha = alg[g];
@@ -570,7 +576,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
           }
         }
 #pragma unroll
-        for (int g = 0; g < kBwdGroup; ++g) {
+        for (int g = 0; g < Lc::kBwdGroup; ++g) {
           if (!__any_sync(0xffffffffu, any[g])) continue;
           // lane 4q ends up with the warp sum of v[q]
           const float s8 = warp_sum8_transposed(v[g], lane);
