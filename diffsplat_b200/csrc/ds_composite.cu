@@ -443,14 +443,17 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   }
   const int32_t warp_final = warp_max(my_final);
   const int nb = (end - start + B - 1) / B;
-  constexpr int R = (B + NT - 1) / NT;  // splats each thread stages
+  // Threads per staged splat: with twice as many threads as batch slots, two
+  // threads share a splat's warp-block tests and its cross-warp sum.
+  constexpr int kSplit = NT >= 2 * B ? 2 : 1;
+  constexpr int R = (B * kSplit + NT - 1) / NT;  // splats each thread stages
   Staged pf[R];
   // batch bi holds sorted indices end - 1 - B bi down to end - B (bi + 1)
   auto prefetch = [&](int bi) {
     const int batch_end = end - 1 - B * bi;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int l = threadIdx.x + r * NT, li = batch_end - l;
+      const int l = (threadIdx.x + r * NT) / kSplit, li = batch_end - l;
       pf[r].ok = l < B && li >= start;
       if (pf[r].ok) {
         const uint32_t g = sorted_splat[li];
@@ -469,18 +472,28 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     // stage the batch back to front: slot l holds sorted index batch_end - l
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int l = threadIdx.x + r * NT;
-      if (l < B) {
-        uint32_t mk = 0u;
-        if (pf[r].ok) {
+      const int slot = threadIdx.x + r * NT, l = slot / kSplit, h = slot % kSplit;
+      uint32_t mk = 0u;
+      if (l < B && pf[r].ok) {
+        if (kSplit == 1) {
+          mk = warp_hits<NW>(pf[r].a, pf[r].b, pf[r].c.w, sBox);
+        } else {
+          // this thread tests half of the warp blocks
+#pragma unroll
+          for (int k = 0; k < NW / 2; ++k) {
+            const int wb = h * (NW / 2) + k;
+            mk |= ellipse_hits(pf[r].a, pf[r].b, pf[r].c.w, sBox[wb]) ? (1u << wb) : 0u;
+          }
+        }
+        if (h == 0) {
           sA[l] = pf[r].a;
           sB[l] = pf[r].b;
           sC[l] = pf[r].c;
           sI[l] = pf[r].idet;
-          mk = warp_hits<NW>(pf[r].a, pf[r].b, pf[r].c.w, sBox);
         }
-        sMask[l] = mk;
       }
+      if (kSplit == 2) mk |= __shfl_xor_sync(0xffffffffu, mk, 1);  // pairs are adjacent lanes
+      if (l < B && h == 0) sMask[l] = mk;
     }
     if (bi + 1 < nb) prefetch(bi + 1);
     {
@@ -587,11 +600,12 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
       }
     }
     __syncthreads();
-    for (int l = threadIdx.x; l < bs; l += NT) {
+    for (int slot = threadIdx.x; slot < bs * kSplit; slot += NT) {
+      const int l = slot / kSplit, h = slot % kSplit;
       const uint32_t e = sorted_emit[batch_end - l];
       float* dst = isect_grad + (size_t)e * 9;
 #pragma unroll
-      for (int q = 0; q < 9; ++q) {
+      for (int q = h; q < 9; q += kSplit) {
         float s = 0.f;
 #pragma unroll
         for (int ww = 0; ww < NW; ++ww) s += part[ww][l * 9 + q];
