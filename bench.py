@@ -139,10 +139,10 @@ NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.393088e6 / 3085768,
 
 def kernels_per_step(tiles: int) -> int:
     passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
-    # step_begin, preprocess, 4 depth passes x 3, scan x 3, emit, tile passes x 3,
+    # step_begin, preprocess, 4 depth passes x 3, scan x 2, emit, tile passes x 3,
     # ranges, tile schedule, composite fwd, composite bwd, long-segment reduce,
     # backward+Adam (which sums the short segments itself)
-    return 2 + 12 + 3 + 1 + 3 * passes + 2 + 4
+    return 2 + 12 + 2 + 1 + 3 * passes + 2 + 4
 
 
 def stage_bytes(n: int, isects: int, pixels: int, tiles: int) -> dict:

@@ -68,7 +68,13 @@ __global__ void __launch_bounds__(kThreads)
                 const unsigned long long* __restrict__ offsets, const ushort4* __restrict__ rect,
                 int n, int ntx, uint32_t cap, uint32_t* __restrict__ tile_keys,
                 uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start,
-                const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom) {
+                const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom,
+                int2* __restrict__ ranges, int tiles) {
+  // The tile ranges of this forward start empty (ranges_kernel fills the
+  // non-empty ones after the tile sort).
+  for (int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x; q < tiles;
+       q += (int64_t)gridDim.x * kThreads)
+    ranges[q] = make_int2(0, 0);
   // Four lanes (a quad) per splat in depth order: they load its count, offset
   // and tile rectangle and write its tiles (row-major over the rectangle) to
   // consecutive emission slots, four at a time.  Splats with more than
@@ -503,7 +509,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
     emit_kernel<<<(unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
         rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
-        rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom);
+        rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom, rb.ranges, rb.tiles);
     DS_CUDA(cudaGetLastError());
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
     // 4) stable sort by tile id; last pass gathers the splat id of each pair
@@ -520,8 +526,8 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
       DS_CUDA(cudaEventRecord(ev[1], s));
     }
   }
-  // 5) per-tile ranges
-  DS_CUDA(cudaMemsetAsync(rb.ranges, 0, (size_t)rb.tiles * sizeof(int2), s));
+  // 5) per-tile ranges (cleared by the emission, or here when nothing was emitted)
+  if (n <= 0) DS_CUDA(cudaMemsetAsync(rb.ranges, 0, (size_t)rb.tiles * sizeof(int2), s));
   {
     const int64_t want = (rb.cap + kThreads - 1) / kThreads;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));

@@ -253,55 +253,63 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads)
-    scan_partials_kernel(unsigned long long* __restrict__ partials,
-                         uint32_t* __restrict__ long_partials, uint32_t cap,
-                         uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
-                         uint32_t* __restrict__ n_long, uint32_t* __restrict__ status) {
-  __shared__ unsigned long long buf[kSortBlocks];
-  __shared__ uint32_t lbuf[kSortBlocks];
-  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) {
-    buf[i] = partials[i];
-    lbuf[i] = long_partials ? long_partials[i] : 0u;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long run = 0;
-    uint32_t lrun = 0;
-    for (int i = 0; i < kSortBlocks; ++i) {
-      const unsigned long long v = buf[i];
-      const uint32_t lv = lbuf[i];
-      buf[i] = run;
-      lbuf[i] = lrun;
-      run += v;
-      lrun += lv;
-    }
-    *raw = run;
-    *n_clamped = (uint32_t)(run < (unsigned long long)cap ? run : cap);
-    if (run > (unsigned long long)cap) atomicOr(status, kStatusIsectOverflow);
-    if (n_long) *n_long = lrun;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kSortBlocks; i += kThreads) {
-    partials[i] = buf[i];
-    if (long_partials) long_partials[i] = lbuf[i];
-  }
-}
-
-__global__ void __launch_bounds__(kThreads)
     scan_final_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
                       uint32_t n, const unsigned long long* __restrict__ partials,
                       unsigned long long* __restrict__ offsets,
                       const uint32_t* __restrict__ long_partials,
-                      uint32_t* __restrict__ long_list) {
-  __shared__ unsigned long long wsum[kWarps];
-  __shared__ uint32_t wlong[kWarps];
+                      uint32_t* __restrict__ long_list, uint32_t cap,
+                      uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
+                      uint32_t* __restrict__ n_long, uint32_t* __restrict__ status) {
+  __shared__ unsigned long long wsum[kWarps], wall[kWarps];
+  __shared__ uint32_t wlong[kWarps], wlall[kWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  // carry = sum of the chunks before this CTA's; CTA 0 also writes the totals
+  unsigned long long carry = 0, all = 0;
+  uint32_t lcarry = 0, lall = 0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) {
+    const unsigned long long v = partials[i];
+    const uint32_t lv = long_list ? long_partials[i] : 0u;
+    if (i < (int)blockIdx.x) {
+      carry += v;
+      lcarry += lv;
+    }
+    all += v;
+    lall += lv;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    carry += __shfl_xor_sync(0xffffffffu, carry, o);
+    lcarry += __shfl_xor_sync(0xffffffffu, lcarry, o);
+    all += __shfl_xor_sync(0xffffffffu, all, o);
+    lall += __shfl_xor_sync(0xffffffffu, lall, o);
+  }
+  if (lane == 0) {
+    wsum[w] = carry;
+    wlong[w] = lcarry;
+    wall[w] = all;
+    wlall[w] = lall;
+  }
+  __syncthreads();
+  carry = all = 0;
+  lcarry = lall = 0;
+#pragma unroll
+  for (int k = 0; k < kWarps; ++k) {
+    carry += wsum[k];
+    lcarry += wlong[k];
+    all += wall[k];
+    lall += wlall[k];
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *raw = all;
+    *n_clamped = (uint32_t)(all < (unsigned long long)cap ? all : cap);
+    if (all > (unsigned long long)cap) atomicOr(status, kStatusIsectOverflow);
+    if (n_long) *n_long = lall;
+  }
   const uint32_t chunk = scan_chunk(n);
   const uint32_t begin = min(blockIdx.x * chunk, n);
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
-  unsigned long long carry = partials[blockIdx.x];
-  uint32_t lcarry = long_list ? long_partials[blockIdx.x] : 0u;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (uint32_t t0 = begin; t0 < end; t0 += kThreads * kScanItems) {
     uint32_t c[kScanItems];
     unsigned long long s = 0;
@@ -398,10 +406,9 @@ int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t 
   if (long_list && (!scratch.long_partials || !n_long)) return DS_ERR_ARG;
   uint32_t* lp = long_list ? scratch.long_partials : nullptr;
   scan_partial_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, lp);
-  scan_partials_kernel<<<1, kThreads, 0, s>>>(scratch.partials, lp, cap, n_clamped, raw_total,
-                                              long_list ? n_long : nullptr, status);
   scan_final_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, offsets,
-                                                     lp, long_list);
+                                                     lp, long_list, cap, n_clamped, raw_total,
+                                                     long_list ? n_long : nullptr, status);
   return cuda_status(cudaGetLastError());
 }
 
