@@ -232,6 +232,10 @@ def call(fn: str, *args) -> None:
     check(fn, getattr(lib(), fn)(*args))
 
 
-def fptr(values) -> C.Array:
-    arr = (C.c_float * len(values))(*[float(v) for v in values])
-    return arr
+def fptr(values):
+    """float * of `values` for one call: a C-contiguous float32 NumPy array is
+    passed in place (the pointer keeps it alive), anything else is copied."""
+    if type(values).__module__ == "numpy" and values.dtype.char == "f" \
+            and values.flags.c_contiguous:
+        return values.ctypes.data_as(_fp)
+    return (C.c_float * len(values))(*[float(v) for v in values])

@@ -59,6 +59,7 @@ struct ds_fitter {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int host_steps = 0;
+  float* loss_host = nullptr;  // pinned slot of the loss read-back
 };
 
 namespace ds {
@@ -167,6 +168,7 @@ int ds_fitter_destroy(ds_fitter* f) {
   cudaFree(f->cam_dev);
   cudaFree(f->bc_table);
   cudaFree(f->bc_cur);
+  if (f->loss_host) cudaFreeHost(f->loss_host);
   delete f;
   return DS_OK;
 }
@@ -317,8 +319,11 @@ int ds_fitter_step(ds_fitter* f, int n_steps, ds_stream stream) {
 int ds_fitter_loss(ds_fitter* f, float* loss, ds_stream stream) {
   if (!f || !loss) return DS_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  DS_CUDA(cudaMemcpyAsync(loss, &f->rb.scalars->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (!f->loss_host) DS_CUDA(cudaHostAlloc((void**)&f->loss_host, sizeof(float), cudaHostAllocDefault));
+  DS_CUDA(cudaMemcpyAsync(f->loss_host, &f->rb.scalars->loss, sizeof(float),
+                          cudaMemcpyDeviceToHost, s));
   DS_CUDA(cudaStreamSynchronize(s));
+  *loss = *f->loss_host;
   return DS_OK;
 }
 
