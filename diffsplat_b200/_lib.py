@@ -18,6 +18,7 @@ DS_ERR_CUDA = 3
 DS_ERR_ISECT_OVERFLOW = 4
 DS_ERR_STATE = 5
 DS_ERR_NO_DEVICE = 6
+DS_ERR_INTERNAL = 7
 
 DS_GRAD_REFERENCE = 0
 DS_GRAD_EXACT = 1

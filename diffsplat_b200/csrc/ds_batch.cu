@@ -394,7 +394,7 @@ int ds_batch_status(ds_batch* b, uint32_t* flags) {
   DS_CUDA(cudaMemcpy(&st, &b->rb.scalars->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   DS_CUDA(cudaMemcpy(&b->rb.scalars->status, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
   *flags = st;
-  return (st & ds::kStatusIsectOverflow) ? DS_ERR_ISECT_OVERFLOW : DS_OK;
+  return ds::status_code(st);
 }
 
 }  // extern "C"

@@ -198,7 +198,7 @@ int ds_raster_status(ds_raster* r, uint32_t* flags) {
   DS_CUDA(cudaMemcpy(&st, &r->rb.scalars->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   DS_CUDA(cudaMemcpy(&r->rb.scalars->status, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
   *flags = st;
-  return (st & ds::kStatusIsectOverflow) ? DS_ERR_ISECT_OVERFLOW : DS_OK;
+  return ds::status_code(st);
 }
 
 int ds_raster_download(ds_raster* r, int what, void* host, int64_t bytes) {

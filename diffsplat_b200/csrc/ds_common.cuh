@@ -43,11 +43,6 @@ __host__ __device__ inline int sh_bands(int degree) {
   return n;
 }
 
-// Sticky error bits written by kernels into a device status word.
-enum StatusBits : uint32_t {
-  kStatusIsectOverflow = 1u << 0,  // more (tile, splat) pairs than the buffer holds
-};
-
 // ---------------------------------------------------------------------------
 // Quaternion / rotation (parity)
 // ---------------------------------------------------------------------------

@@ -346,7 +346,7 @@ int ds_fitter_status(ds_fitter* f, uint32_t* flags) {
   DS_CUDA(cudaMemcpy(&st, &f->rb.scalars->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   DS_CUDA(cudaMemcpy(&f->rb.scalars->status, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
   *flags = st;
-  return (st & ds::kStatusIsectOverflow) ? DS_ERR_ISECT_OVERFLOW : DS_OK;
+  return ds::status_code(st);
 }
 
 int ds_fitter_profile_step(ds_fitter* f, float* stage_ms, int n_stages, ds_stream stream) {

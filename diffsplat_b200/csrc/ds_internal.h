@@ -40,6 +40,19 @@ struct HostStage {
   void release();
 };
 
+// Sticky error bits written by kernels into a device status word.
+enum StatusBits : uint32_t {
+  kStatusIsectOverflow = 1u << 0,  // more (tile, splat) pairs than the buffer holds
+  kStatusBadTile = 1u << 1,        // a sorted pair's tile id lies outside the grid
+};
+
+// Status code for sticky StatusBits read back by a status call.
+inline int status_code(uint32_t bits) {
+  if (bits & kStatusIsectOverflow) return DS_ERR_ISECT_OVERFLOW;
+  if (bits & kStatusBadTile) return DS_ERR_INTERNAL;
+  return DS_OK;
+}
+
 // Layer kernels (ds_activ_project.cu)
 int launch_activ_forward(const ds_gaussian3d& in, int degree, const float cam[3],
                          const ds_splat3d& out, cudaStream_t s);

@@ -259,13 +259,17 @@ int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStre
 
 __global__ void __launch_bounds__(kThreads)
     ranges_kernel(const uint32_t* __restrict__ sorted_tile, const uint32_t* __restrict__ n_dev,
-                  int* __restrict__ ranges) {
+                  int* __restrict__ ranges, uint32_t tiles, uint32_t* __restrict__ status) {
   // ranges[t] = [first, last + 1) of tile t in the sorted pairs, from the
   // boundaries between neighbouring ids (grid-stride; the ranges of tiles with
   // no pair stay (0, 0) from the memset before).
   const uint32_t n = *n_dev;
   for (uint32_t q = blockIdx.x * kThreads + threadIdx.x; q < n; q += gridDim.x * kThreads) {
     const uint32_t t = sorted_tile[q];
+    if (t >= tiles) {  // self-check: never for a correct sort; no write outside ranges
+      atomicOr(status, kStatusBadTile);
+      continue;
+    }
     if (q == 0 || sorted_tile[q - 1] != t) ranges[2 * (size_t)t] = (int)q;
     if (q + 1 == n || sorted_tile[q + 1] != t) ranges[2 * (size_t)t + 1] = (int)(q + 1);
   }
@@ -532,7 +536,8 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     const int64_t want = (rb.cap + kThreads - 1) / kThreads;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
     ranges_kernel<<<blocks, kThreads, 0, s>>>(rb.sorted_tile, &sc->n_isects,
-                                              reinterpret_cast<int*>(rb.ranges));
+                                              reinterpret_cast<int*>(rb.ranges),
+                                              (uint32_t)rb.tiles, &sc->status);
   }
   DS_CUDA(cudaGetLastError());
   if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST) {

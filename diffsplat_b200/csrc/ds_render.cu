@@ -177,7 +177,7 @@ int ds_renderer_status(ds_renderer* r, uint32_t* flags) {
   DS_CUDA(cudaMemcpy(&st, &r->rb.scalars->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   DS_CUDA(cudaMemcpy(&r->rb.scalars->status, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice));
   *flags = st;
-  return (st & ds::kStatusIsectOverflow) ? DS_ERR_ISECT_OVERFLOW : DS_OK;
+  return ds::status_code(st);
 }
 
 int ds_renderer_destroy(ds_renderer* r) {

@@ -36,6 +36,7 @@ extern "C" {
 #define DS_ERR_ISECT_OVERFLOW 4 /* more (tile, splat) pairs than the intersection buffer holds */
 #define DS_ERR_STATE 5          /* call made in the wrong state (e.g. step before set_target) */
 #define DS_ERR_NO_DEVICE 6      /* no CUDA device, or not an sm_100 device */
+#define DS_ERR_INTERNAL 7       /* a device-side consistency check failed (results of the step invalid) */
 
 /* Storage modes for ds_fitter. */
 #define DS_STORAGE_FP32 0 /* all attributes, SH and Adam moments in FP32 */
