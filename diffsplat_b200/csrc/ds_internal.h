@@ -102,12 +102,13 @@ struct ScanScratch {
   uint32_t* long_partials = nullptr;       // [kSortBlocks]; only for the long list
 };
 // offsets[p] = exclusive sum of counts[perm[q]], q < p.  With long_list set,
-// also long_list[0 .. *n_long) = the positions p with counts[perm[p]] >
-// kSerialRecords, ascending.
+// also long_list[0 .. *n_long) = {perm[p], offsets[p], offsets[p] +
+// counts[perm[p]]} (offsets clamped to cap) for the positions p with
+// counts[perm[p]] > kSerialRecords, ascending in p.
 int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
                          unsigned long long* offsets, uint32_t* n_clamped,
                          unsigned long long* raw_total, uint32_t cap, uint32_t* status,
-                         ScanScratch& scratch, cudaStream_t s, uint32_t* long_list = nullptr,
+                         ScanScratch& scratch, cudaStream_t s, uint4* long_list = nullptr,
                          uint32_t* n_long = nullptr);
 
 // Device-resident scalars of one rasterizer / fitter.
@@ -162,7 +163,7 @@ struct RasterBuffers {
   ushort4* rect = nullptr;     // tile rectangle {x0, x1, y0, y1}
   uint32_t* counts = nullptr;  // tiles per splat (0 = invisible)
   uint32_t* seg_start = nullptr;  // first emission index of each splat
-  uint32_t* long_list = nullptr;  // depth-order positions of splats with long record segments
+  uint4* long_list = nullptr;  // {splat, first record, record end} of splats with long segments
   uint32_t* depth_keys = nullptr;  // depth key of each splat (0xffffffff when invisible)
   uint32_t* depth_k0 = nullptr;    // ping-pong buffers of the depth sort
   uint32_t* depth_k1 = nullptr;

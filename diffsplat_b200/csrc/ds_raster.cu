@@ -217,20 +217,17 @@ __global__ void __launch_bounds__(kThreads)
 
 template <bool kAccumulate>
 __global__ void __launch_bounds__(kThreads)
-    segment_reduce_long_kernel(const float* __restrict__ isect_grad,
-                               const uint32_t* __restrict__ perm,
-                               const unsigned long long* __restrict__ offsets,
-                               const uint32_t* __restrict__ counts, uint32_t cap, int n,
+    segment_reduce_long_kernel(const float* __restrict__ isect_grad, int n,
                                float* __restrict__ g2, ds_splat2d gin,
-                               const uint32_t* __restrict__ long_list,
+                               const uint4* __restrict__ long_list,
                                DevScalars* __restrict__ sc) {
   const int lane = threadIdx.x & 31;
   const uint32_t total = sc->n_long;
   for (uint32_t w = (uint32_t)((blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5); w < total;
        w += (uint32_t)(gridDim.x * (kThreads / 32))) {
-    uint32_t i, c;
-    unsigned long long s, e;
-    segment_of(perm, offsets, counts, cap, (int)long_list[w], i, c, s, e);
+    const uint4 seg = long_list[w];
+    const uint32_t i = seg.x;
+    const unsigned long long s = seg.y, e = seg.z;
     float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float a = 0.f;
     for (unsigned long long q = s + lane; q < e; q += 32) {
@@ -251,9 +248,8 @@ template <bool kAccumulate>
 int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStream_t s) {
   const int64_t warps = std::min<int64_t>(n, kLongWarps);
   const unsigned blocks = (unsigned)((warps * 32 + kThreads - 1) / kThreads);
-  segment_reduce_long_kernel<kAccumulate><<<blocks, kThreads, 0, s>>>(
-      rb.isect_grad, rb.depth_perm, rb.emit_offsets, rb.counts, (uint32_t)rb.cap, n, rb.g2, gin,
-      rb.long_list, rb.scalars);
+  segment_reduce_long_kernel<kAccumulate><<<blocks, kThreads, 0, s>>>(rb.isect_grad, n, rb.g2, gin,
+                                                                     rb.long_list, rb.scalars);
   return cuda_status(cudaGetLastError());
 }
 

@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kThreads)
                       uint32_t n, const unsigned long long* __restrict__ partials,
                       unsigned long long* __restrict__ offsets,
                       const uint32_t* __restrict__ long_partials,
-                      uint32_t* __restrict__ long_list, uint32_t cap,
+                      uint4* __restrict__ long_list, uint32_t cap,
                       uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
                       uint32_t* __restrict__ n_long, uint32_t* __restrict__ status) {
   __shared__ unsigned long long wsum[kWarps], wall[kWarps];
@@ -311,13 +311,14 @@ __global__ void __launch_bounds__(kThreads)
   const uint32_t end = min(begin + chunk, n);
   if (begin >= end) return;
   for (uint32_t t0 = begin; t0 < end; t0 += kThreads * kScanItems) {
-    uint32_t c[kScanItems];
+    uint32_t c[kScanItems], pi[kScanItems];
     unsigned long long s = 0;
     uint32_t lmask = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
       uint32_t p = t0 + threadIdx.x * kScanItems + k;
-      c[k] = p < end ? counts[perm[p]] : 0u;
+      pi[k] = p < end ? perm[p] : 0u;
+      c[k] = p < end ? counts[pi[k]] : 0u;
       s += c[k];
       lmask |= (c[k] > kSerialRecords ? 1u : 0u) << k;
     }
@@ -356,9 +357,15 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
       uint32_t p = t0 + threadIdx.x * kScanItems + k;
-      if (p < end) offsets[p] = excl;
+      const unsigned long long s0 = excl;
+      if (p < end) offsets[p] = s0;
       excl += c[k];
-      if (long_list && (lmask >> k & 1u)) long_list[lexcl++] = p;
+      if (long_list && (lmask >> k & 1u)) {
+        // {splat, first record, end of its records}, clamped to the capacity
+        const unsigned long long cp = cap;
+        long_list[lexcl++] = make_uint4(pi[k], (uint32_t)(s0 < cp ? s0 : cp),
+                                        (uint32_t)(excl < cp ? excl : cp), 0u);
+      }
     }
     carry += tot;
     lcarry += ltot;
@@ -401,7 +408,7 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
 int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t n,
                          unsigned long long* offsets, uint32_t* n_clamped,
                          unsigned long long* raw_total, uint32_t cap, uint32_t* status,
-                         ScanScratch& scratch, cudaStream_t s, uint32_t* long_list,
+                         ScanScratch& scratch, cudaStream_t s, uint4* long_list,
                          uint32_t* n_long) {
   if (long_list && (!scratch.long_partials || !n_long)) return DS_ERR_ARG;
   uint32_t* lp = long_list ? scratch.long_partials : nullptr;
