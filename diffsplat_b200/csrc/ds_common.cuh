@@ -43,6 +43,11 @@ __host__ __device__ inline int sh_bands(int degree) {
   return n;
 }
 
+// Waits until the kernel this one was launched after with programmatic
+// dependent launch (launch_pdl) has completed and its writes are visible; a
+// no-op for an ordinary launch.  Kernels of the step chain call it first.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // Quaternion / rotation (parity)
 // ---------------------------------------------------------------------------

@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                          const uint16_t* __restrict__ tile_inst, const InstGeom* __restrict__ geom,
                          const float* __restrict__ target, float* __restrict__ loss_partials,
                          DevScalars* __restrict__ sc) {
+  pdl_wait();
   using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
   constexpr int NW = Lc::kWarps;
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                          float* __restrict__ isect_grad, int W_, int H_, int ntx_,
                          const uint16_t* __restrict__ tile_inst,
                          const InstGeom* __restrict__ geom) {
+  pdl_wait();
   using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
   constexpr int NW = Lc::kWarps;
@@ -625,10 +627,10 @@ void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, bool cou
   constexpr int NT = Lay<PPT, TS>::kThreads;
   const int32_t* order = schedule(rb);
 #define DS_FWD(L, C)                                                                         \
-  composite_fwd_kernel<PPT, TS, L, C, kBatch><<<rb.tiles, NT, 0, s>>>(                       \
-      rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb, rb.alphas,   \
-      rb.last_ids, rb.width, rb.height, rb.ntx, rb.tile_inst, rb.geom, L ? target : nullptr, \
-      L ? rb.loss_partials : nullptr, rb.scalars)
+  launch_pdl(composite_fwd_kernel<PPT, TS, L, C, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
+             rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb,        \
+             rb.alphas, rb.last_ids, rb.width, rb.height, rb.ntx, rb.tile_inst, rb.geom,      \
+             L ? target : nullptr, L ? rb.loss_partials : nullptr, rb.scalars)
   if (count) DS_FWD(false, true);
   else if (target) DS_FWD(true, false);
   else DS_FWD(false, false);
@@ -644,10 +646,10 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
   const bool exact = rb.grad_mode == DS_GRAD_EXACT;
   const int32_t* order = schedule(rb);
 #define DS_BWD(F, E)                                                                         \
-  composite_bwd_kernel<PPT, TS, F, E, kBatch><<<rb.tiles, NT, 0, s>>>(                       \
-      rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit, rb.ranges, \
-      order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width, rb.height, rb.ntx,       \
-      rb.tile_inst, rb.geom)
+  launch_pdl(composite_bwd_kernel<PPT, TS, F, E, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
+             rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit,      \
+             rb.ranges, order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width,         \
+             rb.height, rb.ntx, rb.tile_inst, rb.geom)
   if (grad_rgb) {
     if (exact) DS_BWD(false, true);
     else DS_BWD(false, false);

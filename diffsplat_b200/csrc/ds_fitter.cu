@@ -72,19 +72,20 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   RasterBuffers& rb = f->rb;
   const int n = f->cfg.count;
   if (ev) DS_CUDA(cudaEventRecord(ev[0], s));
-  step_begin_kernel<<<1, 1, 0, s>>>(rb.scalars, f->bc_table, f->bc_len, f->bc_cur);
-  DS_CUDA(cudaGetLastError());
+  DS_CUDA(launch_pdl(step_begin_kernel, dim3(1), dim3(1), 0, s, rb.scalars, f->bc_table, f->bc_len,
+                     f->bc_cur));
   const int blocks = (n + kThreads - 1) / kThreads;
   const bool bf16 = f->cfg.storage == DS_STORAGE_BF16;
   if (bf16)
-    fit_preprocess_kernel<<<blocks, kThreads, 0, s>>>(
-        f->P, f->R16, f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx, rb.nty,
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
+    DS_CUDA(launch_pdl(fit_preprocess_kernel<__nv_bfloat16>, dim3(blocks), dim3(kThreads), 0, s,
+                       f->P, f->R16, f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx,
+                       rb.nty, rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts,
+                       rb.depth_keys, rb.scalars, nullptr, nullptr));
   else
-    fit_preprocess_kernel<<<blocks, kThreads, 0, s>>>(
-        f->P, soa_of(f->P), f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx, rb.nty,
-        rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts, rb.depth_keys, rb.scalars);
-  DS_CUDA(cudaGetLastError());
+    DS_CUDA(launch_pdl(fit_preprocess_kernel<float>, dim3(blocks), dim3(kThreads), 0, s, f->P,
+                       soa_of(f->P), f->cfg.sh_degree, f->cam_dev, rb.width, rb.height, rb.ntx,
+                       rb.nty, rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.rect, rb.counts,
+                       rb.depth_keys, rb.scalars, nullptr, nullptr));
   if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
   DS_TRY(raster_build_lists(rb, n, s, ev ? ev + 2 : nullptr, true));
   DS_TRY(raster_composite_forward(rb, f->image, f->target, s));
@@ -97,16 +98,15 @@ static int fitter_enqueue(ds_fitter* f, cudaStream_t s, cudaEvent_t* ev = nullpt
   AdamHyper h{f->cfg.beta1, f->cfg.beta2, f->cfg.epsilon};
   const int keep = f->g_mem ? 1 : 0, exact = f->cfg.grad_mode == DS_GRAD_EXACT ? 1 : 0;
   if (bf16)
-    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
-        f->P, f->R16, f->M16, f->V16, f->G, keep, exact, f->cfg.sh_degree, f->cam_dev, rb.g2,
-        grad_segments(rb), f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum,
-        f->grad_count);
+    DS_CUDA(launch_pdl(fit_backward_adam_kernel<__nv_bfloat16>, dim3(blocks), dim3(kThreads), 0,
+                       s, f->P, f->R16, f->M16, f->V16, f->G, keep, exact, f->cfg.sh_degree,
+                       f->cam_dev, rb.g2, grad_segments(rb), f->bc_cur, rb.scalars, lr, h,
+                       nullptr, rb.counts, f->grad_accum, f->grad_count));
   else
-    fit_backward_adam_kernel<<<blocks, kThreads, 0, s>>>(
-        f->P, soa_of(f->P), soa_of(f->M), soa_of(f->V), f->G, keep, exact, f->cfg.sh_degree,
-        f->cam_dev, rb.g2, grad_segments(rb), f->bc_cur, rb.scalars, lr, h, nullptr, rb.counts,
-        f->grad_accum, f->grad_count);
-  DS_CUDA(cudaGetLastError());
+    DS_CUDA(launch_pdl(fit_backward_adam_kernel<float>, dim3(blocks), dim3(kThreads), 0, s, f->P,
+                       soa_of(f->P), soa_of(f->M), soa_of(f->V), f->G, keep, exact,
+                       f->cfg.sh_degree, f->cam_dev, rb.g2, grad_segments(rb), f->bc_cur,
+                       rb.scalars, lr, h, nullptr, rb.counts, f->grad_accum, f->grad_count));
   if (ev) DS_CUDA(cudaEventRecord(ev[7], s));
   return DS_OK;
 }

@@ -25,6 +25,7 @@ struct Lrs {
 
 __global__ void step_begin_kernel(DevScalars* sc, const float2* __restrict__ bc_table,
                                   int table_len, float2* __restrict__ bc_out) {
+  pdl_wait();
   uint32_t t = sc->step + 1u;
   sc->step = t;
   sc->visible = 0u;
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(kThreads)
                              const uint32_t* __restrict__ visible = nullptr,
                              float* __restrict__ grad_accum = nullptr,
                              uint32_t* __restrict__ grad_count = nullptr) {
+  pdl_wait();
   constexpr bool kBf16 = sizeof(T) == 2;
   __shared__ Mat4 sP;
   __shared__ float sCam[3];

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/diffsplat_b200.h"
 
 namespace ds {
@@ -20,6 +22,25 @@ inline int cuda_status(cudaError_t e) {
   } while (0)
 
 #define DS_CUDA(expr) DS_TRY(::ds::cuda_status(expr))
+
+// Launches `kernel` with programmatic dependent launch: its CTAs may be
+// scheduled while the previous kernel in the stream finishes, and it waits
+// for that kernel (pdl_wait) before its first memory access.
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, A&&... args) {
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 // Small host -> device uploads (cameras) through a ring of pinned slots
 // (ds_stage.cu): an upload waits only for the copy that used its slot kSlots

@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(kPreThreads)
                           DevScalars* __restrict__ sc,
                           const uint16_t* __restrict__ inst_of_splat = nullptr,
                           const InstGeom* __restrict__ geom = nullptr) {
+  pdl_wait();
   __shared__ Mat4 sP;
   __shared__ float sCam[3];
   if (!kBatch) {

@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(kThreads)
                 uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start,
                 const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom,
                 int2* __restrict__ ranges, int tiles) {
+  pdl_wait();
   // The tile ranges of this forward start empty (ranges_kernel fills the
   // non-empty ones after the tile sort).
   for (int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x; q < tiles;
@@ -221,6 +222,7 @@ __global__ void __launch_bounds__(kThreads)
                                float* __restrict__ g2, ds_splat2d gin,
                                const uint4* __restrict__ long_list,
                                DevScalars* __restrict__ sc) {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const uint32_t total = sc->n_long;
   for (uint32_t w = (uint32_t)((blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5); w < total;
@@ -248,14 +250,15 @@ template <bool kAccumulate>
 int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStream_t s) {
   const int64_t warps = std::min<int64_t>(n, kLongWarps);
   const unsigned blocks = (unsigned)((warps * 32 + kThreads - 1) / kThreads);
-  segment_reduce_long_kernel<kAccumulate><<<blocks, kThreads, 0, s>>>(rb.isect_grad, n, rb.g2, gin,
-                                                                     rb.long_list, rb.scalars);
+  DS_CUDA(launch_pdl(segment_reduce_long_kernel<kAccumulate>, dim3(blocks), dim3(kThreads), 0, s,
+                     rb.isect_grad, n, rb.g2, gin, rb.long_list, rb.scalars));
   return cuda_status(cudaGetLastError());
 }
 
 __global__ void __launch_bounds__(kThreads)
     ranges_kernel(const uint32_t* __restrict__ sorted_tile, const uint32_t* __restrict__ n_dev,
                   int* __restrict__ ranges, uint32_t tiles, uint32_t* __restrict__ status) {
+  pdl_wait();
   // ranges[t] = [first, last + 1) of tile t in the sorted pairs, from the
   // boundaries between neighbouring ids (grid-stride; the ranges of tiles with
   // no pair stay (0, 0) from the memset before).
@@ -287,6 +290,7 @@ __device__ __forceinline__ int work_bucket(int2 r) {
 
 __global__ void __launch_bounds__(1024)
     tile_order_kernel(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
+  pdl_wait();
   __shared__ uint32_t cnt[kOrderBuckets];
   __shared__ uint32_t off[kOrderBuckets];
   for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0u;
@@ -507,10 +511,10 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
                                 &sc->n_isects, &sc->n_isects_raw, (uint32_t)rb.cap, &sc->status,
                                 rb.scan, s, with_long_list ? rb.long_list : nullptr, &sc->n_long));
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
-    emit_kernel<<<(unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-        rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
-        rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom, rb.ranges, rb.tiles);
-    DS_CUDA(cudaGetLastError());
+    DS_CUDA(launch_pdl(emit_kernel, dim3((unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads)),
+                       dim3(kThreads), 0, s, rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect,
+                       n, rb.ntx, (uint32_t)rb.cap, rb.tile_k0, rb.emit_splat, rb.seg_start,
+                       rb.inst_of_splat, rb.geom, rb.ranges, rb.tiles));
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
     // 4) stable sort by tile id; last pass gathers the splat id of each pair
     DS_TRY(radix_sort_pairs(rb.tile_k0, nullptr, rb.tile_k1, rb.tile_v1, rb.tile_k0, rb.tile_v0,
@@ -531,14 +535,14 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
   {
     const int64_t want = (rb.cap + kThreads - 1) / kThreads;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
-    ranges_kernel<<<blocks, kThreads, 0, s>>>(rb.sorted_tile, &sc->n_isects,
-                                              reinterpret_cast<int*>(rb.ranges),
-                                              (uint32_t)rb.tiles, &sc->status);
+    DS_CUDA(launch_pdl(ranges_kernel, dim3(blocks), dim3(kThreads), 0, s, rb.sorted_tile,
+                       &sc->n_isects, reinterpret_cast<int*>(rb.ranges), (uint32_t)rb.tiles,
+                       &sc->status));
   }
   DS_CUDA(cudaGetLastError());
   if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST) {
-    tile_order_kernel<<<1, 1024, 0, s>>>(rb.ranges, rb.tiles, rb.tile_order);
-    DS_CUDA(cudaGetLastError());
+    DS_CUDA(launch_pdl(tile_order_kernel, dim3(1), dim3(1024), 0, s, rb.ranges, rb.tiles,
+                       rb.tile_order));
   }
   if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
   return DS_OK;

@@ -35,6 +35,7 @@ __device__ __forceinline__ uint32_t sort_chunk(uint32_t n, uint32_t G) {
 __global__ void __launch_bounds__(kThreads)
     radix_hist_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ n_dev,
                       uint32_t cap, int shift, uint32_t* __restrict__ hist) {
+  pdl_wait();
   __shared__ uint32_t h[256];
   const uint32_t G = gridDim.x;
   const uint32_t n = min(*n_dev, cap);
@@ -71,6 +72,7 @@ __global__ void __launch_bounds__(kThreads)
 constexpr int kRowChunks = (kSortBlocks + 31) / 32;
 
 __global__ void __launch_bounds__(kThreads) scan_hist_kernel(uint32_t* __restrict__ hist, int G) {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int d = blockIdx.x * kWarps + (threadIdx.x >> 5);
   uint32_t* row = hist + (size_t)d * G;
@@ -106,6 +108,7 @@ __global__ void __launch_bounds__(kThreads)
                          const uint32_t* __restrict__ n_dev, uint32_t cap, int shift,
                          const uint32_t* __restrict__ offs, const uint32_t* __restrict__ gsrc,
                          uint32_t* __restrict__ gdst) {
+  pdl_wait();
   __shared__ uint32_t cnt[kWarps][256];  // per-warp digit counts, then per-warp offsets
   __shared__ uint32_t gbase[256];        // output position of the tile's first item of a digit
   __shared__ uint32_t lstart[256];       // tile-local start of each digit
@@ -218,6 +221,7 @@ __global__ void __launch_bounds__(kThreads)
     scan_partial_kernel(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ perm,
                         uint32_t n, unsigned long long* __restrict__ partials,
                         uint32_t* __restrict__ long_partials) {
+  pdl_wait();
   __shared__ unsigned long long wsum[kWarps];
   __shared__ uint32_t wlong[kWarps];
   const uint32_t chunk = scan_chunk(n);
@@ -260,6 +264,7 @@ __global__ void __launch_bounds__(kThreads)
                       uint4* __restrict__ long_list, uint32_t cap,
                       uint32_t* __restrict__ n_clamped, unsigned long long* __restrict__ raw,
                       uint32_t* __restrict__ n_long, uint32_t* __restrict__ status) {
+  pdl_wait();
   __shared__ unsigned long long wsum[kWarps], wall[kWarps];
   __shared__ uint32_t wlong[kWarps], wlall[kWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -390,11 +395,14 @@ int radix_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* ka, uin
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     const bool last = p == passes - 1;
-    radix_hist_kernel<<<G, kThreads, 0, s>>>(src_k, n_dev, cap, shift, scratch.hist);
-    scan_hist_kernel<<<256 / kWarps, kThreads, 0, s>>>(scratch.hist, G);
-    radix_scatter_kernel<<<G, kThreads, 0, s>>>(
-        src_k, src_v, src_v == nullptr ? 1 : 0, dst_k, dst_v, n_dev, cap, shift, scratch.hist,
-        last ? gather_src : nullptr, last ? gather_dst : nullptr);
+    DS_CUDA(launch_pdl(radix_hist_kernel, dim3(G), dim3(kThreads), 0, s, src_k, n_dev, cap, shift,
+                       scratch.hist));
+    DS_CUDA(launch_pdl(scan_hist_kernel, dim3(256 / kWarps), dim3(kThreads), 0, s, scratch.hist,
+                       G));
+    DS_CUDA(launch_pdl(radix_scatter_kernel, dim3(G), dim3(kThreads), 0, s, src_k, src_v,
+                       src_v == nullptr ? 1 : 0, dst_k, dst_v, n_dev, cap, shift,
+                       (const uint32_t*)scratch.hist, last ? gather_src : nullptr,
+                       last ? gather_dst : nullptr));
     *out_k = dst_k;
     *out_v = dst_v;
     src_k = dst_k;
@@ -412,10 +420,11 @@ int scan_counts_permuted(const uint32_t* counts, const uint32_t* perm, uint32_t 
                          uint32_t* n_long) {
   if (long_list && (!scratch.long_partials || !n_long)) return DS_ERR_ARG;
   uint32_t* lp = long_list ? scratch.long_partials : nullptr;
-  scan_partial_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, lp);
-  scan_final_kernel<<<kSortBlocks, kThreads, 0, s>>>(counts, perm, n, scratch.partials, offsets,
-                                                     lp, long_list, cap, n_clamped, raw_total,
-                                                     long_list ? n_long : nullptr, status);
+  DS_CUDA(launch_pdl(scan_partial_kernel, dim3(kSortBlocks), dim3(kThreads), 0, s, counts, perm,
+                     n, scratch.partials, lp));
+  DS_CUDA(launch_pdl(scan_final_kernel, dim3(kSortBlocks), dim3(kThreads), 0, s, counts, perm, n,
+                     (const unsigned long long*)scratch.partials, offsets, (const uint32_t*)lp,
+                     long_list, cap, n_clamped, raw_total, long_list ? n_long : nullptr, status));
   return cuda_status(cudaGetLastError());
 }
 
