@@ -77,6 +77,7 @@ const char* ds_status_string(int status) {
     case DS_ERR_ISECT_OVERFLOW: return "intersection buffer overflow";
     case DS_ERR_STATE: return "invalid state";
     case DS_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case DS_ERR_INTERNAL: return "device-side consistency check failed";
     default: return "unknown status";
   }
 }

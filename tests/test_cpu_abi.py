@@ -30,6 +30,8 @@ def test_status_strings_and_version():
     from diffsplat_b200 import _lib as L
     assert L.lib().ds_abi_version() == 1
     assert L.lib().ds_status_string(L.DS_ERR_ISECT_OVERFLOW) == b"intersection buffer overflow"
+    assert L.lib().ds_status_string(L.DS_ERR_INTERNAL) == b"device-side consistency check failed"
+    assert L.lib().ds_status_string(99) == b"unknown status"
 
 
 def test_ctypes_struct_layouts_match_header(tmp_path):
