@@ -398,6 +398,51 @@ __device__ __forceinline__ float warp_sum8_transposed(const float (&v)[8], int l
   return z;
 }
 
+// Two hits' 8 values each, reduced over the warp at once: after the first
+// exchange (xor 16) lanes 0-15 carry hit 0 and lanes 16-31 hit 1, then the
+// 8-value transposed tree runs within each half.  Even lane l ends up with
+// the warp sum of value (l >> 1) & 7 of hit l >> 4.
+__device__ __forceinline__ float warp_sum16_transposed(const float (&v0)[8], const float (&v1)[8],
+                                                       int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+  float u[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float keep = b4 ? v1[k] : v0[k];
+    const float send = b4 ? v0[k] : v1[k];
+    u[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float keep = b3 ? u[k + 4] : u[k];
+    const float send = b3 ? u[k] : u[k + 4];
+    w[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  float x[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float keep = b2 ? w[k + 2] : w[k];
+    const float send = b2 ? w[k] : w[k + 2];
+    x[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  const float keep = b1 ? x[1] : x[0];
+  const float send = b1 ? x[0] : x[1];
+  float z = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+
+// Two values' warp sums at once: lanes 0-15 end with the sum of a0, lanes
+// 16-31 with the sum of a1.
+__device__ __forceinline__ float warp_sum2_transposed(float a0, float a1, int lane) {
+  const bool b4 = lane & 16;
+  float z = (b4 ? a1 : a0) + __shfl_xor_sync(0xffffffffu, b4 ? a0 : a1, 16);
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+  return z;
+}
+
 // Position gradient through the position dependence of J (Cov2D = J S J^T),
 // which the reference's projection backward leaves out.  H is dL/dCov2D in the
 // full-matrix convention (off-diagonal = stored gradient / 2), S the 3D

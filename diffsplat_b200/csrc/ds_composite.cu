@@ -590,14 +590,26 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
             T[k] = T_before;
           }
         }
+        bool hit_any[Lc::kBwdGroup];
 #pragma unroll
-        for (int g = 0; g < Lc::kBwdGroup; ++g) {
-          if (!__any_sync(0xffffffffu, any[g])) continue;
-          // lane 4q ends up with the warp sum of v[q]
-          const float s8 = warp_sum8_transposed(v[g], lane);
-          const float sa = warp_sum(va[g]);
-          if ((lane & 3) == 0) part[w][tg[g] * 9 + (lane >> 2)] = s8;
-          if (lane == 0) part[w][tg[g] * 9 + 8] = sa;
+        for (int g = 0; g < Lc::kBwdGroup; ++g) hit_any[g] = __any_sync(0xffffffffu, any[g]);
+        if (Lc::kBwdGroup == 2 && hit_any[0] && hit_any[Lc::kBwdGroup - 1]) {
+          // both hits contributed: one butterfly for their 2 x 9 sums
+          const float s16 = warp_sum16_transposed(v[0], v[Lc::kBwdGroup - 1], lane);
+          const float s2 = warp_sum2_transposed(va[0], va[Lc::kBwdGroup - 1], lane);
+          const int gh = lane >> 4;
+          if ((lane & 1) == 0) part[w][tg[gh] * 9 + ((lane >> 1) & 7)] = s16;
+          if ((lane & 15) == 0) part[w][tg[gh] * 9 + 8] = s2;
+        } else {
+#pragma unroll
+          for (int g = 0; g < Lc::kBwdGroup; ++g) {
+            if (!hit_any[g]) continue;
+            // lane 4q ends up with the warp sum of v[q]
+            const float s8 = warp_sum8_transposed(v[g], lane);
+            const float sa = warp_sum(va[g]);
+            if ((lane & 3) == 0) part[w][tg[g] * 9 + (lane >> 2)] = s8;
+            if (lane == 0) part[w][tg[g] * 9 + 8] = sa;
+          }
         }
       }
     }
