@@ -419,7 +419,8 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   const Pixels<PPT> m = pixels<PPT, TS>(tg.local, tg.ntx, W, H);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
-  float T[PPT], gr[PPT], gg[PPT], gb[PPT], accr[PPT], accg[PPT], accb[PPT];
+  // acc[k]: over the splats behind (already visited), weight x (colour . dL/dpixel)
+  float T[PPT], gr[PPT], gg[PPT], gb[PPT], acc[PPT];
   int32_t fin[PPT];
   int32_t my_final = -1;
 #pragma unroll
@@ -441,7 +442,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
         gb[k] = grad_or_image[pix * 3 + 2];
       }
     }
-    accr[k] = accg[k] = accb[k] = 0.f;
+    acc[k] = 0.f;
   }
   const int32_t warp_final = warp_max(my_final);
   const int nb = (end - start + B - 1) / B;
@@ -568,25 +569,28 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
             v[g][2] += fac * gb[k];
             // Reference recurrence (tile_rasterize_layer.cu:518-521) weighs the
             // colour behind (absolute weights c_j alpha_j T_j) by T_before; the
-            // exact derivative divides it by T_after instead.
+            // exact derivative divides it by T_after instead.  The three
+            // colour channels enter only through their dot product with
+            // dL/dpixel.
+            const float cg_k = c.x * gr[k] + c.y * gg[k] + c.z * gb[k];
             const float ia = kExact ? 1.f / T[k] : 1.f;
-            const float v_alpha = T_before * ((c.x - accr[k] * ia) * gr[k] +
-                                              (c.y - accg[k] * ia) * gg[k] +
-                                              (c.z - accb[k] * ia) * gb[k]);
+            const float v_alpha = T_before * (cg_k - acc[k] * ia);
             if (opac * g_exp <= kMaxAlpha) {
               va[g] += g_exp * v_alpha;
-              const float v_dist2 = 0.5f * (-opac * g_exp * v_alpha);
-              const float ddx = 2.f * (dx * b.x + dy * b.y);
-              const float ddy = 2.f * (dx * b.y + dy * b.z);
-              v[g][3] += v_dist2 * ddx;
-              v[g][4] += v_dist2 * ddy;
-              v[g][5] += v_dist2 * (-0.25f * ddx * ddx);
-              v[g][7] += v_dist2 * (-0.25f * ddy * ddy);
-              v[g][6] += v_dist2 * (-2.f * b.y * dist2 - 2.f * dx * dy * ig[g]);
+              // s = -2 dL/d(dist2).  With u = dx bx + dy by and w = dx by + dy
+              // bz, d dist2 / d(ndc x, ndc y) = (2u, 2w) and d dist2 / d(conic)
+              // gives the Cov2D terms -u^2, -w^2 and -2 (by dist2 + dx dy idet).
+              const float s = opac * g_exp * v_alpha;
+              const float u = dx * b.x + dy * b.y;
+              const float wv = dx * b.y + dy * b.z;
+              v[g][3] -= s * u;
+              v[g][4] -= s * wv;
+              const float hs = 0.5f * s;
+              v[g][5] += hs * u * u;
+              v[g][7] += hs * wv * wv;
+              v[g][6] += s * (b.y * dist2 + dx * dy * ig[g]);
             }
-            accr[k] += c.x * fac;
-            accg[k] += c.y * fac;
-            accb[k] += c.z * fac;
+            acc[k] += cg_k * fac;
             T[k] = T_before;
           }
         }
