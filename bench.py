@@ -131,10 +131,10 @@ FLOPS_PER_PAIR = {"composite_fwd": 24, "composite_bwd": 70}
 
 # DRAM bytes (read + write) per (tile, splat) pair of one composite launch, from
 # one ncu capture of the same 1280x720 / 60000-splat workload (profile run, step
-# 21, about 3,085,768 pairs: forward 22.42 MB, backward 184.63 MB), scaled by
+# 21, about 3,085,768 pairs: forward 22.42 MB, backward 184.27 MB), scaled by
 # the bench's own pair count.
 NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.42176e6 / 3085768,
-                            "composite_bwd": 184.62976e6 / 3085768}
+                            "composite_bwd": 184.27365e6 / 3085768}
 
 
 def kernels_per_step(tiles: int) -> int:
