@@ -171,7 +171,7 @@ def cpu_baseline_oracle(prob, budget_s: float = 10.0) -> dict:
     while steps == 0 or time.perf_counter() - t0 < budget_s:
         fw, gp = O.loss_and_grads(P, prob.sh_degree, prob.cam, prob.pv, prob.width, prob.height,
                                   prob.target, threads=threads)
-        P, m, v = O.adam(P, gp, m, v, 1e-3, steps + 1)
+        P, m, v = O.adam_gaussian3d(P, gp, m, v, prob.lrs, steps + 1)
         steps += 1
     dt = time.perf_counter() - t0
     return {"value": steps / dt, "unit": "steps/s", "cores": threads, "kind": "port",

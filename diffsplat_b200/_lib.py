@@ -121,6 +121,7 @@ _SIGS = {
     "ds_raster_download": (C.c_int, [_vp, C.c_int, _vp, C.c_int64]),
     "ds_raster_destroy": (C.c_int, [_vp]),
     "ds_raster_forward_noalloc": (C.c_int, [C.POINTER(Splat2D), C.c_int, C.c_int, _vp, _vp]),
+    "ds_raster_noalloc_status": (C.c_int, [C.POINTER(C.c_uint32), _vp]),
     "ds_mse_forward": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp]),
     "ds_mse_backward": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp]),
     "ds_adam_step": (C.c_int, [C.POINTER(AdamGroup), C.c_int, C.c_float, C.c_float, C.c_float,
@@ -143,6 +144,7 @@ _SIGS = {
     "ds_fitter_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "ds_fitter_pair_stats": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int, _vp]),
     "ds_fitter_params_updated": (C.c_int, [_vp]),
+    "ds_fitter_download": (C.c_int, [_vp, C.c_int, _vp, C.c_int64]),
     "ds_fitter_densify": (C.c_int, [_vp, C.POINTER(DensifyParams), C.POINTER(C.c_int32), _vp]),
     "ds_fitter_density_stats": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
     "ds_batch_default_config": (C.c_int, [C.POINTER(BatchConfig)]),

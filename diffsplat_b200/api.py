@@ -361,6 +361,20 @@ class Fitter:
         L.call("ds_fitter_counters", self.h, out, 3)
         return {"n_isects": int(out[0]), "visible": int(out[1]), "step": int(out[2])}
 
+    def download(self, what: int) -> np.ndarray:
+        """Tile lists / per-pixel state of the most recent step's forward (the
+        DS_RASTER_* codes of Rasterizer.download)."""
+        n = min(self.counters()["n_isects"], 1 << 31)
+        px = self.width * self.height
+        tiles = ((self.width + 15) // 16) * ((self.height + 15) // 16)
+        spec = {L.DS_RASTER_KEYS: (np.uint64, n), L.DS_RASTER_IDS: (np.uint32, n),
+                L.DS_RASTER_RANGES: (np.int32, 2 * tiles),
+                L.DS_RASTER_LAST_IDS: (np.int32, px), L.DS_RASTER_ALPHAS: (np.float32, px),
+                L.DS_RASTER_COUNTS: (np.uint32, self.count)}[what]
+        arr = np.zeros(max(spec[1], 1), spec[0])
+        L.call("ds_fitter_download", self.h, what, arr.ctypes.data, arr.nbytes)
+        return arr[:spec[1]]
+
     def pair_stats(self) -> dict:
         """(pixel, splat) pairs of the most recent step's composite: those that
         contribute and those the kernel evaluates."""

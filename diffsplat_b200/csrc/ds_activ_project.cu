@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(ds_splat3d in, Mat4 P,
 }
 
 // dL/dCov3D = J^T H J with H = [[gxx, gxy/2], [gxy/2, gyy]] and dL/dpos = J^T dndc_xy
-// (persp_project_layer.cu:275-298).
+// (persp_project_layer.cu:244-260).
 struct ProjGrad {
   float px, py, pz, cxx, cxy, cxz, cyy, cyz, czz;
 };

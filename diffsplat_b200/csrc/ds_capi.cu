@@ -204,48 +204,7 @@ int ds_raster_status(ds_raster* r, uint32_t* flags) {
 
 int ds_raster_download(ds_raster* r, int what, void* host, int64_t bytes) {
   if (!r || !host || bytes < 0) return DS_ERR_ARG;
-  ds::RasterBuffers& rb = r->rb;
-  DS_CUDA(cudaDeviceSynchronize());
-  uint32_t n = 0;
-  DS_CUDA(cudaMemcpy(&n, &rb.scalars->n_isects, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  const size_t px = (size_t)rb.width * rb.height;
-  switch (what) {
-    case DS_RASTER_KEYS: {
-      if ((size_t)bytes < (size_t)n * 8) return DS_ERR_ARG;
-      if (n == 0) return DS_OK;
-      std::vector<uint32_t> tiles(n), ids(n), depth(r->last_count > 0 ? r->last_count : 1);
-      DS_CUDA(cudaMemcpy(tiles.data(), rb.sorted_tile, n * 4, cudaMemcpyDeviceToHost));
-      DS_CUDA(cudaMemcpy(ids.data(), rb.sorted_splat, n * 4, cudaMemcpyDeviceToHost));
-      DS_CUDA(cudaMemcpy(depth.data(), rb.depth_keys, (size_t)r->last_count * 4,
-                         cudaMemcpyDeviceToHost));
-      uint64_t* k = (uint64_t*)host;
-      for (uint32_t q = 0; q < n; ++q) k[q] = ((uint64_t)tiles[q] << 32) | depth[ids[q]];
-      return DS_OK;
-    }
-    case DS_RASTER_IDS:
-      if ((size_t)bytes < (size_t)n * 4) return DS_ERR_ARG;
-      if (n) DS_CUDA(cudaMemcpy(host, rb.sorted_splat, (size_t)n * 4, cudaMemcpyDeviceToHost));
-      return DS_OK;
-    case DS_RASTER_RANGES:
-      if ((size_t)bytes < (size_t)rb.tiles * 8) return DS_ERR_ARG;
-      DS_CUDA(cudaMemcpy(host, rb.ranges, (size_t)rb.tiles * 8, cudaMemcpyDeviceToHost));
-      return DS_OK;
-    case DS_RASTER_LAST_IDS:
-      if ((size_t)bytes < px * 4) return DS_ERR_ARG;
-      DS_CUDA(cudaMemcpy(host, rb.last_ids, px * 4, cudaMemcpyDeviceToHost));
-      return DS_OK;
-    case DS_RASTER_ALPHAS:
-      if ((size_t)bytes < px * 4) return DS_ERR_ARG;
-      DS_CUDA(cudaMemcpy(host, rb.alphas, px * 4, cudaMemcpyDeviceToHost));
-      return DS_OK;
-    case DS_RASTER_COUNTS:
-      if ((size_t)bytes < (size_t)r->last_count * 4) return DS_ERR_ARG;
-      if (r->last_count)
-        DS_CUDA(cudaMemcpy(host, rb.counts, (size_t)r->last_count * 4, cudaMemcpyDeviceToHost));
-      return DS_OK;
-    default:
-      return DS_ERR_ARG;
-  }
+  return ds::raster_download(r->rb, r->last_count, what, host, bytes);
 }
 
 int ds_raster_destroy(ds_raster* r) {

@@ -237,7 +237,7 @@ struct Cov2 {
   float xx, xy, yy;
 };
 
-// Cov2D = J Cov3D J^T, upper triangle (persp_project_layer.cu:164-180).
+// Cov2D = J Cov3D J^T, upper triangle (persp_project_layer.cu:131-142).
 __device__ __forceinline__ Cov2 cov2_from(const Jac2& J, float cxx, float cxy, float cxz, float cyy,
                                           float cyz, float czz) {
   float js00 = dot3_b(J.j00, cxx, J.j01, cxy, J.j02, cxz);

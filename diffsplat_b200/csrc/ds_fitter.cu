@@ -394,6 +394,12 @@ int ds_fitter_pair_stats(ds_fitter* f, uint64_t* out, int n, ds_stream stream) {
   return DS_OK;
 }
 
+int ds_fitter_download(ds_fitter* f, int what, void* host, int64_t bytes) {
+  if (!f || !host || bytes < 0) return DS_ERR_ARG;
+  if (f->host_steps == 0) return DS_ERR_STATE;
+  return ds::raster_download(f->rb, f->cfg.count, what, host, bytes);
+}
+
 // Test hook: a fitter that also writes the Gaussian3D gradients of each step.
 int ds_fitter_create_with_grads(const ds_fitter_config* cfg, ds_fitter** out) {
   return ds_fitter_create_impl(cfg, 1, out);

@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kThreads)
     grad_count[i] += 1u;
   }
 
-  // 2) projection backward (persp_project_layer.cu:245-305)
+  // 2) projection backward (persp_project_layer.cu:173-267)
   const float px = P.pos_x[i], py = P.pos_y[i], pz = P.pos_z[i];
   const float rw = ldv(R.rot_w[i]), rx = ldv(R.rot_x[i]), ry = ldv(R.rot_y[i]),
               rz = ldv(R.rot_z[i]);

@@ -103,12 +103,15 @@ const uint16_t kDistBase[30] = {1,    2,    3,    4,    5,    7,     9,     13, 
 const uint8_t kDistExtra[30] = {0, 0, 0, 0, 1, 1, 2, 2,  3,  3,  4,  4,  5,  5,  6,
                                 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
 
+// Output beyond `limit` bytes fails the decode: a small crafted stream could
+// otherwise expand to gigabytes before the size check of its caller.
 bool inflate_block(BitReader& br, const Huffman& lit, const Huffman& dist,
-                   std::vector<uint8_t>& out) {
+                   std::vector<uint8_t>& out, size_t limit) {
   for (;;) {
     int sym = lit.decode(br);
     if (sym < 0 || br.bad) return false;
     if (sym < 256) {
+      if (out.size() >= limit) return false;
       out.push_back((uint8_t)sym);
     } else if (sym == 256) {
       return true;
@@ -119,14 +122,14 @@ bool inflate_block(BitReader& br, const Huffman& lit, const Huffman& dist,
       const int ds = dist.decode(br);
       if (ds < 0 || ds >= 30) return false;
       const size_t d = kDistBase[ds] + br.bits(kDistExtra[ds]);
-      if (d > out.size()) return false;
+      if (d > out.size() || out.size() + (size_t)len > limit) return false;
       const size_t from = out.size() - d;
       for (int i = 0; i < len; ++i) out.push_back(out[from + i]);
     }
   }
 }
 
-bool inflate(const uint8_t* data, size_t n, std::vector<uint8_t>& out) {
+bool inflate(const uint8_t* data, size_t n, std::vector<uint8_t>& out, size_t limit) {
   BitReader br{data, n};
   int last = 0;
   do {
@@ -138,7 +141,7 @@ bool inflate(const uint8_t* data, size_t n, std::vector<uint8_t>& out) {
       const uint16_t len = (uint16_t)(data[br.pos] | (data[br.pos + 1] << 8));
       const uint16_t nlen = (uint16_t)(data[br.pos + 2] | (data[br.pos + 3] << 8));
       br.pos += 4;
-      if ((uint16_t)~nlen != len || br.pos + len > n) return false;
+      if ((uint16_t)~nlen != len || br.pos + len > n || out.size() + len > limit) return false;
       out.insert(out.end(), data + br.pos, data + br.pos + len);
       br.pos += len;
     } else if (type == 1) {  // fixed Huffman codes
@@ -151,7 +154,7 @@ bool inflate(const uint8_t* data, size_t n, std::vector<uint8_t>& out) {
       Huffman lit, dist;
       lit.build(l, 288);
       dist.build(d, 30);
-      if (!inflate_block(br, lit, dist, out)) return false;
+      if (!inflate_block(br, lit, dist, out, limit)) return false;
     } else if (type == 2) {  // dynamic Huffman codes
       const int hlit = (int)br.bits(5) + 257, hdist = (int)br.bits(5) + 1;
       const int hclen = (int)br.bits(4) + 4;
@@ -186,7 +189,7 @@ bool inflate(const uint8_t* data, size_t n, std::vector<uint8_t>& out) {
       }
       Huffman lit, dist;
       if (!lit.build(lens, hlit) || !dist.build(lens + hlit, hdist)) return false;
-      if (!inflate_block(br, lit, dist, out)) return false;
+      if (!inflate_block(br, lit, dist, out, limit)) return false;
     } else {
       return false;
     }
@@ -265,7 +268,9 @@ bool decode_png(const std::vector<uint8_t>& f, int* w, int* h, std::vector<uint8
   if (idat.size() < 6) return false;
   std::vector<uint8_t> raw;
   raw.reserve((size_t)(W * ch + 1) * H);
-  if (!inflate(idat.data() + 2, idat.size() - 6, raw)) return false;  // zlib header / Adler-32
+  // zlib header / Adler-32 around the deflate stream; the filtered rows are
+  // (stride + 1) * H bytes, more is malformed
+  if (!inflate(idat.data() + 2, idat.size() - 6, raw, (size_t)(W * ch + 1) * H)) return false;
   const size_t stride = (size_t)W * ch;
   if (raw.size() < (stride + 1) * H) return false;
   std::vector<uint8_t> img(stride * H);

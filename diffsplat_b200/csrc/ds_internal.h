@@ -256,6 +256,11 @@ void raster_free(RasterBuffers& rb);
 int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev = nullptr,
                        bool with_long_list = false);
 
+// Copies the state of the last forward to host memory (synchronises the
+// device); `what` is one of DS_RASTER_KEYS .. DS_RASTER_COUNTS and n_splats the
+// splat count of that forward.
+int raster_download(const RasterBuffers& rb, int n_splats, int what, void* host, int64_t bytes);
+
 // Composite forward.  When target != nullptr the per-tile squared error is
 // also accumulated and reduced into rb.scalars->loss (L = sum / pixels).
 // Forward that also counts (pixel, splat) pairs into scalars->pairs (which it

@@ -17,6 +17,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "ds_common.cuh"
 #include "ds_internal.h"
@@ -546,6 +547,55 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
   }
   if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
   return DS_OK;
+}
+
+int raster_download(const RasterBuffers& rb, int n_splats, int what, void* host, int64_t bytes) {
+  if (!host || bytes < 0 || n_splats < 0) return DS_ERR_ARG;
+  DS_CUDA(cudaDeviceSynchronize());
+  uint32_t n = 0;
+  DS_CUDA(cudaMemcpy(&n, &rb.scalars->n_isects, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  const size_t px = (size_t)rb.width * rb.height;
+  switch (what) {
+    case DS_RASTER_KEYS: {
+      // (tile id << 32) | depth bits of the pair's splat, in sorted order
+      if ((size_t)bytes < (size_t)n * 8) return DS_ERR_ARG;
+      if (n == 0) return DS_OK;
+      std::vector<uint32_t> tiles(n), ids(n), depth(n_splats > 0 ? n_splats : 1);
+      DS_CUDA(cudaMemcpy(tiles.data(), rb.sorted_tile, (size_t)n * 4, cudaMemcpyDeviceToHost));
+      DS_CUDA(cudaMemcpy(ids.data(), rb.sorted_splat, (size_t)n * 4, cudaMemcpyDeviceToHost));
+      DS_CUDA(cudaMemcpy(depth.data(), rb.depth_keys, (size_t)n_splats * 4,
+                         cudaMemcpyDeviceToHost));
+      uint64_t* k = (uint64_t*)host;
+      for (uint32_t q = 0; q < n; ++q) {
+        if (ids[q] >= (uint32_t)n_splats) return DS_ERR_INTERNAL;
+        k[q] = ((uint64_t)tiles[q] << 32) | depth[ids[q]];
+      }
+      return DS_OK;
+    }
+    case DS_RASTER_IDS:
+      if ((size_t)bytes < (size_t)n * 4) return DS_ERR_ARG;
+      if (n) DS_CUDA(cudaMemcpy(host, rb.sorted_splat, (size_t)n * 4, cudaMemcpyDeviceToHost));
+      return DS_OK;
+    case DS_RASTER_RANGES:
+      if ((size_t)bytes < (size_t)rb.tiles * 8) return DS_ERR_ARG;
+      DS_CUDA(cudaMemcpy(host, rb.ranges, (size_t)rb.tiles * 8, cudaMemcpyDeviceToHost));
+      return DS_OK;
+    case DS_RASTER_LAST_IDS:
+      if ((size_t)bytes < px * 4) return DS_ERR_ARG;
+      DS_CUDA(cudaMemcpy(host, rb.last_ids, px * 4, cudaMemcpyDeviceToHost));
+      return DS_OK;
+    case DS_RASTER_ALPHAS:
+      if ((size_t)bytes < px * 4) return DS_ERR_ARG;
+      DS_CUDA(cudaMemcpy(host, rb.alphas, px * 4, cudaMemcpyDeviceToHost));
+      return DS_OK;
+    case DS_RASTER_COUNTS:
+      if ((size_t)bytes < (size_t)n_splats * 4) return DS_ERR_ARG;
+      if (n_splats)
+        DS_CUDA(cudaMemcpy(host, rb.counts, (size_t)n_splats * 4, cudaMemcpyDeviceToHost));
+      return DS_OK;
+    default:
+      return DS_ERR_ARG;
+  }
 }
 
 int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStream_t s) {

@@ -11,7 +11,9 @@
 //
 // Per pass (8-bit digit), three kernels:
 //   hist    : per-CTA digit histogram of its contiguous chunk -> hist[digit][cta]
-//   scan    : one CTA turns the digit-major histogram into exclusive offsets
+//   scan    : 32 CTAs, one warp per digit row, scan the digit-major
+//             histogram into per-CTA exclusive offsets and row totals (the
+//             scatter adds the prefix of the 256 digit totals itself)
 //   scatter : each CTA re-reads its chunk 2048 items at a time, ranks items
 //             stably inside each warp with __match_any_sync, combines warp
 //             counts in shared memory and writes every item to its slot.

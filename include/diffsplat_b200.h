@@ -116,7 +116,7 @@ int ds_activ_backward(const ds_gaussian3d *in, const ds_splat3d *out, const ds_s
                       ds_stream stream);
 
 /* ---- Projection: replaces PerspProjectLayer::forward / ::backward / ::setCamera
- *      (src/layers/persp_project_layer.cu:316-334, :336-355, :307-312).
+ *      (src/layers/persp_project_layer.cu:278-296, :298-317, :269-274).
  *      pv is the column-major 16-float PV = proj * view that setCamera uploads;
  *      here it is passed per call, so two layers may use different cameras. */
 int ds_project_forward(const ds_splat3d *in, const float pv[16], const ds_splat2d *out,
@@ -177,12 +177,19 @@ int ds_raster_destroy(ds_raster *r);
  * intermediate buffer in one ~5.7 MB __device__ array of the library that each
  * GPU holds until the process exits.  Limits: count <= 8192 splats,
  * width * height <= 65536 pixels, at most 1024 16x16 tiles (DS_ERR_ARG
- * beyond); (tile, splat) pairs beyond 131072 are dropped.  All calls on a
- * device share the array, so calls that overlap on the GPU race: issue them on
- * one stream.  The first call on each device looks up the array's device
- * address; make it before any stream capture.  Asynchronous. */
+ * beyond); (tile, splat) pairs beyond 131072 are dropped, the deepest first,
+ * exactly as ds_raster_forward drops pairs beyond a 131072-pair capacity, and
+ * a sticky overflow bit is set that ds_raster_noalloc_status reports.  All
+ * calls on a device share the array, so calls that overlap on the GPU race:
+ * issue them on one stream.  The first call on each device, and the first
+ * after a device reset, looks up the array's device address; make it before
+ * any stream capture.  Asynchronous. */
 int ds_raster_forward_noalloc(const ds_splat2d *in, int width, int height, float *out_rgb,
                               ds_stream stream);
+/* Reads and clears the sticky status bits of ds_raster_forward_noalloc on the
+ * current device (synchronises `stream`; allocates nothing).  Returns
+ * DS_ERR_ISECT_OVERFLOW when a call since the last read dropped pairs. */
+int ds_raster_noalloc_status(uint32_t *flags, ds_stream stream);
 
 /* ---- Loss: replaces MSELossLayer::forward / ::backward / ::getLoss
  *      (src/layers/mse_loss_layer.cu:85-92, :94-99, :101-105).
@@ -271,6 +278,14 @@ int ds_fitter_counters(ds_fitter *f, uint64_t *out, int n);
  * that contribute (alpha >= 1/255 before the pixel terminates), out[1] = pairs
  * the kernel evaluates.  Rewrites the same image; synchronises. */
 int ds_fitter_pair_stats(ds_fitter *f, uint64_t *out, int n, ds_stream stream);
+/* Copies the tile lists and per-pixel state of the most recent step's forward
+ * to host memory (synchronises the device), with the codes and layouts of
+ * ds_raster_download (DS_RASTER_KEYS .. DS_RASTER_COUNTS).  That forward ran on
+ * the parameters as they were before the step's Adam update.  No reference
+ * counterpart: the reference keeps these lists inside TileRasterizeLayer
+ * (src/layers/tile_rasterize_layer.h:23-60); this hook lets a test compare the
+ * fused step's lists with the layer path's. */
+int ds_fitter_download(ds_fitter *f, int what, void *host, int64_t bytes);
 int ds_fitter_grads(ds_fitter *f, ds_gaussian3d *out);
 int ds_fitter_moments(ds_fitter *f, ds_gaussian3d *m, ds_gaussian3d *v);
 

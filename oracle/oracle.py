@@ -177,6 +177,24 @@ def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):
     return p, m, v
 
 
+def adam_gaussian3d(p, g, m, v, lrs, step, b1=0.9, b2=0.999, eps=1e-8):
+    """Adam over a field-major Gaussian3D parameter array [14 + 3K, n] with the
+    per-group learning rates lrs = (pos, scale, rot, sh_dc, sh_rest, opacity)
+    of registerGaussian3DGroups (src/optimizers/gaussian3d_adam.h:27-55)."""
+    p, m, v = _f64(p).copy(), _f64(m).copy(), _f64(v).copy()
+    g = _f64(g)
+    rows = p.shape[0]
+    groups = [(0, 3, lrs[0]), (3, 6, lrs[1]), (6, 10, lrs[2]), (10, 13, lrs[3]),
+              (13, 14, lrs[5])] + ([(14, rows, lrs[4])] if rows > 14 else [])
+    for a, b, lr in groups:
+        pa, ma, va = p[a:b].copy(), m[a:b].copy(), v[a:b].copy()
+        ga = np.ascontiguousarray(g[a:b])
+        lib().orc_adam(pa.size, pa.reshape(-1), ga.reshape(-1), ma.reshape(-1), va.reshape(-1),
+                       float(lr), b1, b2, eps, step)
+        p[a:b], m[a:b], v[a:b] = pa, ma, va
+    return p, m, v
+
+
 @dataclass
 class Forward:
     S3: np.ndarray

@@ -90,3 +90,14 @@ def test_first_adam_step(case):
         z = np.zeros_like(P[r])
         after[r], _, _ = O.adam(P[r], GP[r], z, z, lr[r], 1)
     assert (np.abs(after - d["params_after_adam"]) / lr[:, None]).max() < 1e-3
+
+
+def test_first_adam_step_grouped(case):
+    """The grouped oracle Adam (the CPU baseline's optimizer) applies the
+    registerGaussian3DGroups learning rates row by row, like the reference's
+    Adam::step on the golden fixture."""
+    _, d, *_, P, _, GP = case
+    lr = _row_lrs(d["lrs"], P.shape[0])
+    z = np.zeros_like(P)
+    after, _, _ = O.adam_gaussian3d(P, GP, z, z, tuple(float(x) for x in d["lrs"]), 1)
+    assert (np.abs(after - d["params_after_adam"]) / lr[:, None]).max() < 1e-3

@@ -73,3 +73,34 @@ def test_errors(tmp_path):
     PIL.fromarray(a).save(jpg)
     with pytest.raises(L.DSError):
         api.read_image(jpg)
+
+
+def _png_chunk(kind: bytes, data: bytes) -> bytes:
+    import struct
+    import zlib
+    return struct.pack(">I", len(data)) + kind + data + struct.pack(
+        ">I", zlib.crc32(kind + data) & 0xFFFFFFFF)
+
+
+def test_png_stream_expanding_past_the_image_is_rejected(tmp_path):
+    """A tiny IDAT that inflates far beyond the (stride + 1) * H bytes its
+    header announces fails the decode instead of expanding in memory."""
+    import struct
+    import zlib
+    W = H = 4
+    ihdr = struct.pack(">IIBBBBB", W, H, 8, 2, 0, 0, 0)
+    bomb = zlib.compress(b"\0" * (64 << 20), 9)  # 64 MiB of zeros in about 64 KB
+    assert len(bomb) < (1 << 17)
+    png = b"\x89PNG\r\n\x1a\n" + _png_chunk(b"IHDR", ihdr) + _png_chunk(b"IDAT", bomb) + \
+        _png_chunk(b"IEND", b"")
+    path = tmp_path / "bomb.png"
+    path.write_bytes(png)
+    with pytest.raises(L.DSError):
+        api.read_image(path)
+    # the same header with exactly its rows decodes
+    rows = b"".join(b"\0" + bytes(range(3 * W)) for _ in range(H))
+    ok = b"\x89PNG\r\n\x1a\n" + _png_chunk(b"IHDR", ihdr) + _png_chunk(
+        b"IDAT", zlib.compress(rows)) + _png_chunk(b"IEND", b"")
+    path.write_bytes(ok)
+    img = api.read_image(path)
+    assert img.shape == (H, W, 3) and np.array_equal(img[0].reshape(-1), np.arange(3 * W))

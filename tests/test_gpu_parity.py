@@ -144,7 +144,7 @@ def test_raster_vs_fp64_oracle(runs, name):
 @pytest.mark.parametrize("name", ["96x64_sh0", "160x90_sh3"])
 def test_exact_gradient_mode_vs_fp64_oracle(cuda_lib, name):
     """DS_GRAD_EXACT is the true derivative; the FP64 oracle in exact mode agrees
-    with FP64 central differences (tests/test_oracle_cpu.py)."""
+    with FP64 central differences (tests/test_cpu_oracle.py)."""
     from oracle import oracle as O
     prob = dict(PROBLEMS)[name]()
     me = ds_layers(prob, grad_mode=1)
