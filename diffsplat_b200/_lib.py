@@ -34,6 +34,7 @@ DS_RASTER_RANGES = 2
 DS_RASTER_LAST_IDS = 3
 DS_RASTER_ALPHAS = 4
 DS_RASTER_COUNTS = 5
+DS_RASTER_CONICS = 6
 
 _fp = C.POINTER(C.c_float)
 _vp = C.c_void_p

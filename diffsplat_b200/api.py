@@ -200,7 +200,8 @@ class Rasterizer:
         spec = {L.DS_RASTER_KEYS: (np.uint64, n), L.DS_RASTER_IDS: (np.uint32, n),
                 L.DS_RASTER_RANGES: (np.int32, 2 * self.tiles),
                 L.DS_RASTER_LAST_IDS: (np.int32, px), L.DS_RASTER_ALPHAS: (np.float32, px),
-                L.DS_RASTER_COUNTS: (np.uint32, n_splats)}[what]
+                L.DS_RASTER_COUNTS: (np.uint32, n_splats),
+                L.DS_RASTER_CONICS: (np.float32, 4 * n_splats)}[what]
         arr = np.zeros(max(spec[1], 1), spec[0])
         L.call("ds_raster_download", self.h, what, arr.ctypes.data, arr.nbytes)
         return arr[:spec[1]]
@@ -370,7 +371,8 @@ class Fitter:
         spec = {L.DS_RASTER_KEYS: (np.uint64, n), L.DS_RASTER_IDS: (np.uint32, n),
                 L.DS_RASTER_RANGES: (np.int32, 2 * tiles),
                 L.DS_RASTER_LAST_IDS: (np.int32, px), L.DS_RASTER_ALPHAS: (np.float32, px),
-                L.DS_RASTER_COUNTS: (np.uint32, self.count)}[what]
+                L.DS_RASTER_COUNTS: (np.uint32, self.count),
+                L.DS_RASTER_CONICS: (np.float32, 4 * self.count)}[what]
         arr = np.zeros(max(spec[1], 1), spec[0])
         L.call("ds_fitter_download", self.h, what, arr.ctypes.data, arr.nbytes)
         return arr[:spec[1]]

@@ -593,6 +593,11 @@ int raster_download(const RasterBuffers& rb, int n_splats, int what, void* host,
       if (n_splats)
         DS_CUDA(cudaMemcpy(host, rb.counts, (size_t)n_splats * 4, cudaMemcpyDeviceToHost));
       return DS_OK;
+    case DS_RASTER_CONICS:
+      if ((size_t)bytes < (size_t)n_splats * 16) return DS_ERR_ARG;
+      if (n_splats)
+        DS_CUDA(cudaMemcpy(host, rb.rec_b, (size_t)n_splats * 16, cudaMemcpyDeviceToHost));
+      return DS_OK;
     default:
       return DS_ERR_ARG;
   }

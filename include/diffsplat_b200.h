@@ -159,13 +159,19 @@ int ds_raster_status(ds_raster *r, uint32_t *flags);
  *   DS_RASTER_RANGES    int32  [2*tiles]   per-tile {start, end}; {0,0} for empty tiles
  *   DS_RASTER_LAST_IDS  int32  [H*W]       sorted-list index of each pixel's last contributor
  *   DS_RASTER_ALPHAS    float  [H*W]       1 - final transmittance
- *   DS_RASTER_COUNTS    uint32 [count]     tiles covered per splat */
+ *   DS_RASTER_COUNTS    uint32 [count]     tiles covered per splat
+ *   DS_RASTER_CONICS    float  [count*4]   per splat {a, b, c, opacity}: the inverse of
+ *                                          its Splat2D covariance [[a, b], [b, c]] as the
+ *                                          compositing evaluates it (reference: computed at
+ *                                          batch load, tile_rasterize_layer.cu:260-272);
+ *                                          meaningful for splats with a non-zero count */
 #define DS_RASTER_KEYS 0
 #define DS_RASTER_IDS 1
 #define DS_RASTER_RANGES 2
 #define DS_RASTER_LAST_IDS 3
 #define DS_RASTER_ALPHAS 4
 #define DS_RASTER_COUNTS 5
+#define DS_RASTER_CONICS 6
 int ds_raster_download(ds_raster *r, int what, void *host, int64_t bytes);
 int ds_raster_destroy(ds_raster *r);
 

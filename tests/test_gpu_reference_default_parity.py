@@ -1,27 +1,55 @@
 """Parity of the fused, graph-captured training step at the size the headline
 metric is quoted on: the reference-default fitter (1280x720 procedural target
 with 2000 blobs, 60000 splats, fx = fy = 1000, SH 0, 16x16 tiles, the
-reference's Adam learning rates).
+reference's Adam learning rates), over 4000 steps.
 
 Every 100 steps the fused fitter's current parameters are pushed through the
 reference's own CUDA layers (oracle/_ref/libdsref.so, wired like
-ImageFitter::step) and the next fused step's forward lists are compared with
-the reference's forward on the same parameters:
+ImageFitter::step) and the next fused step is compared with the reference's
+forward and backward on the same parameters:
 
   * (tile, splat) pair count, visible count, per-splat tile counts, sorted
-    64-bit (tile << 32 | depth bits) keys, sorted splat ids (the reference's
-    ids canonicalised to ascending order within equal keys: its slot order
-    comes from atomicAdd, src/layers/tile_rasterize_layer.cu:138) and tile
-    ranges: bit-exact (tileAssign :52-144, SortPairs :664-684, ranges
-    :148-162);
-  * image: within 1e-5 relative (norm-wise); bit-exact, with the same last
-    contributor ids, in every tile whose list the reference holds in exactly
-    our order (forward :637-708);
-  * Gaussian3D gradients: within 1e-4 relative per field (backward :710-728
-    through the projection and activation backward).
+    64-bit (tile << 32 | depth bits) keys, sorted splat ids and tile ranges:
+    bit-exact (tileAssign src/layers/tile_rasterize_layer.cu:52-144,
+    SortPairs :664-684, ranges :148-162).  The reference's ids are put in
+    ascending order inside runs of equal keys first: its order there is the
+    atomicAdd slot order (:138) and changes from run to run.
+  * Equal keys are common at this size (about 15000 tied neighbours in 3600
+    tiles at the start), and the reference composites a tie in its run's
+    slot order, so its image and gradients differ between two of its own
+    runs (about 2e-4 relative in the image and 3e-3 in the gradients at the
+    start).  The image and the last-contributor ids are therefore compared
+    bit for bit in every tile whose list the reference held in exactly our
+    order (forward :637-708), and the Splat2D gradients of the compositing
+    backward (:356-578) within 1e-4 relative per field over the splats none
+    of whose pairs lies in another tile (3e-4 for the three covariance
+    fields, see COV_TOL).
+  * Our projection and activation backward, given the reference's own
+    Splat2D gradients, reproduce its Gaussian3D gradients within 1e-4
+    relative per field (persp_project_layer.cu:173-267,
+    gauss_activ_layer.cu:198-407), and the fused step's Gaussian3D gradients
+    equal those of the library's layer path on the same parameters within
+    1e-5 (the same per-pair records, summed in another order).
+  * Every 500 steps the whole frame is checked against the FP64 oracle's
+    compositing (oracle/oracle.cpp) over our lists, fed with this step's
+    FP32 Splat2D (the forward with the FP32 conics the compositing
+    evaluates): the image within 1e-5 relative and the last ids exactly
+    (pixels within rounding of a threshold left out, and the one or two
+    pixels a frame where a very elongated splat moves the last contributor),
+    and the layer path's
+    Splat2D gradients within 1e-4 relative per field (3e-4 covariance) of
+    the oracle's FP64 composite backward given the same forward state, over
+    the splats whose screen covariance is not nearly singular (det >= 1e-2
+    cxx cyy): the FP32 1 / det (tile_rasterize_layer.cu:260-272, ours
+    alike) that enters the covariance gradients is off from the FP64 one by
+    about 6e-8 times cxx cyy / det, which nears the tolerance beyond that.
 
-The trajectories themselves are not compared: the fused step sums gradients
-in a fixed order, the reference with float atomics.
+Gaussian3D gradients are not compared with FP64 at this size: for splats
+with a nearly singular screen covariance the activation backward (dM = 2 G M,
+gauss_activ_layer.cu:272-294) cancels large terms, and FP32 -- the
+reference's as much as ours -- departs from FP64 by up to tens of percent on
+single log-scale entries.  The trajectories themselves are not compared: the
+fused step sums gradients in a fixed order, the reference with float atomics.
 """
 import os
 
@@ -33,89 +61,200 @@ from tests.helpers import rel_err
 
 pytestmark = pytest.mark.gpu
 
-IMG_TOL = 1e-5   # image, relative (norm-wise)
-GRAD_TOL = 1e-4  # gradients, relative (norm-wise per field)
+IMG_TOL = 1e-5    # image, relative (norm-wise)
+GRAD_TOL = 1e-4   # gradients, relative (norm-wise per field)
+FUSED_TOL = 1e-5  # fused step vs layer path: the same records, summed in another order
 STEPS = int(os.environ.get("DS_PARITY_STEPS", "4000"))
 EVERY = 100
+ORACLE_EVERY = 500
+SPLAT2D_ROWS = (0, 1, 3, 4, 5, 6, 7, 8, 9)  # ndc z (row 2) carries no gradient
+# Covariance rows of the Splat2D gradient: the reference's formula
+# (tile_rasterize_layer.cu:518-542) subtracts terms of the conic and of
+# dx dy / det that nearly cancel for elongated splats, so once the fit has
+# elongated them its FP32 value carries summation-order noise near 1e-4
+# relative (measured over 4000 steps: ours against the reference up to
+# 1.8e-4, while ours and the reference are equally far from FP64, 1.8e-5 on
+# the same splats).
+COV_ROWS = (3, 4, 5)
+COV_TOL = 3e-4
 
 
-def _same_order_mask(keys, my_ids, ref_raw_ids, W, H):
-    """Pixels of tiles whose list the reference composited in exactly our
-    order (its order inside equal keys follows atomicAdd arrival)."""
-    differ = my_ids != ref_raw_ids
-    bad = np.unique((keys[differ] >> np.uint64(32)).astype(np.int64))
+def _tol(row):
+    return COV_TOL if row in COV_ROWS else GRAD_TOL
+
+
+def _tile_masks(keys, my_ids, ref_raw_ids, W, H, n_tiles):
+    """Tiles the reference composited in an order other than ours (its order
+    inside equal keys follows atomicAdd arrival), and the pixels of the
+    other tiles."""
+    tile_of = (keys >> np.uint64(32)).astype(np.int64)
+    bad = np.zeros(n_tiles, bool)
+    bad[tile_of[my_ids != ref_raw_ids]] = True
     ntx = (W + 15) // 16
     ok = np.ones((H, W), bool)
-    for t in bad:
+    for t in np.flatnonzero(bad):
         ty, tx = divmod(int(t), ntx)
         ok[ty * 16:(ty + 1) * 16, tx * 16:(tx + 1) * 16] = False
-    return ok
+    return tile_of, bad, ok
 
 
 def test_fused_fitter_lists_image_grads_vs_reference_every_100_steps(cuda_lib):
     import torch
     from diffsplat_b200 import _lib as L
     from diffsplat_b200 import api
+    from oracle import oracle as O
     from oracle import ref
     if not ref.available():
         pytest.skip("oracle/_ref/libdsref.so not built (needs the reference sources)")
     prob = reference_default(seed=0)
     W, H, n = prob.width, prob.height, prob.params.shape[1]
     assert (W, H, n, prob.sh_degree) == (1280, 720, 60000, 0)
+    n_tiles = ((W + 15) // 16) * ((H + 15) // 16)
+    tgt = torch.tensor(prob.target, device="cuda")
     f = api.Fitter(W, H, n, 0, lrs=prob.lrs, keep_grads=True)
     f.set_params(prob.params)
-    f.set_target(torch.tensor(prob.target, device="cuda"))
+    f.set_target(tgt)
     f.set_camera(prob.pv, prob.cam)
     R = ref.RefScene(W, H, prob.params, 0, prob.target, prob.pv, prob.cam, prob.lrs)
-    checked = 0
-    worst_img, worst_grad, same_frac = 0.0, 0.0, 1.0
+    raster = api.Rasterizer(W, H, n, 1 << 25)
+    checked, same_frac, ill_max, flips_max = 0, 1.0, 0, 0
+    worst = {"splat2d_ref": 0.0, "splat2d_cov_ref": 0.0, "g3d_ref": 0.0, "fused": 0.0,
+             "img_fp64": 0.0, "splat2d_fp64": 0.0, "splat2d_cov_fp64": 0.0,
+             "splat2d_cov_ours_fp64": 0.0, "splat2d_cov_ref_fp64": 0.0}
     for c in range(0, STEPS, EVERY):
+        where = f"after {c} steps"
         P = f.params.cpu().numpy().copy()  # parameters after c steps
         f.step(1)                          # step c + 1: forward on P, backward, Adam
+        cnt = f.counters()
         mine = dict(
-            n_isects=f.counters()["n_isects"], visible=f.counters()["visible"],
             keys=f.download(L.DS_RASTER_KEYS), ids=f.download(L.DS_RASTER_IDS),
             ranges=f.download(L.DS_RASTER_RANGES), counts=f.download(L.DS_RASTER_COUNTS),
             last_ids=f.download(L.DS_RASTER_LAST_IDS).reshape(H, W),
-            image=f.image().cpu().numpy(), grads=f.grads().cpu().numpy(), loss=f.loss())
+            image=f.image().cpu().numpy(), grads=f.grads().cpu().numpy())
+        # the reference's layers on the same parameters
         R.set_params(P)
         R.zero_grad()
         R.forward()
-        loss = R.loss()
         R.backward()
         raw_keys, raw_ids = R.download(0), R.download(1)
         keys, ids = ref.canonical_order(raw_keys, raw_ids)
-        where = f"after {c} steps"
-        assert mine["n_isects"] == R.n_isects() > 0, where
-        assert mine["visible"] == R.visible(), where
+        assert np.array_equal(raw_keys, keys), where  # the reference's keys come sorted
+        # lists: bit-exact
+        assert cnt["n_isects"] == R.n_isects() > 0, where
+        assert cnt["visible"] == R.visible(), where
         assert np.array_equal(mine["keys"], keys), where
         assert np.array_equal(mine["ids"], ids), where
         assert np.array_equal(mine["ranges"], R.download(2)), where
-        # per-splat tile counts, from the reference's sorted ids
-        ref_counts = np.bincount(ids, minlength=n).astype(np.uint32)
-        assert np.array_equal(mine["counts"], ref_counts), where
-        img = R.download(3)
-        e = rel_err(mine["image"], img)
-        worst_img = max(worst_img, e)
-        assert e <= IMG_TOL, where
-        assert np.array_equal(raw_keys, keys), where  # the reference's keys come sorted
-        ok = _same_order_mask(keys, mine["ids"], raw_ids, W, H)
+        assert np.array_equal(mine["counts"], np.bincount(ids, minlength=n)), where
+        # image and last ids: bit-exact where the reference used our order
+        tile_of, bad, ok = _tile_masks(keys, mine["ids"], raw_ids, W, H, n_tiles)
         same_frac = min(same_frac, ok.mean())
-        assert np.array_equal(mine["image"][ok].view(np.uint32), img[ok].view(np.uint32)), where
+        assert ok.any(), where
+        ref_img = R.download(3)
+        assert np.array_equal(mine["image"][ok].view(np.uint32), ref_img[ok].view(np.uint32)), \
+            where
         assert np.array_equal(mine["last_ids"][ok], R.download(5)[ok]), where
-        assert abs(mine["loss"] - loss) <= 1e-5 * loss, where
-        GP = R.download(6)
-        for row in range(GP.shape[0]):
-            e = rel_err(mine["grads"][row], GP[row])
-            worst_grad = max(worst_grad, e)
-            assert e <= GRAD_TOL, f"{where}: Gaussian3D row {row}"
+        # the library's layer path on the same parameters: same image, and the
+        # Splat2D gradients the fused step reduces internally
+        Pt = torch.tensor(P, device="cuda")
+        S3g = api.activ_forward(Pt, 0, prob.cam)
+        S2g = api.project_forward(S3g, prob.pv)
+        img2 = raster.forward(S2g)
+        assert np.array_equal(img2.cpu().numpy(), mine["image"]), where
+        G2t = raster.backward(S2g, api.mse_backward(img2, tgt))
+        GPg = api.activ_backward(Pt, S3g, api.project_backward(S3g, prob.pv, G2t), 0,
+                                 prob.cam).cpu().numpy()
+        G2g = G2t.cpu().numpy()
+        for row in range(GPg.shape[0]):
+            e = rel_err(mine["grads"][row], GPg[row])
+            worst["fused"] = max(worst["fused"], e)
+            assert e <= FUSED_TOL, f"{where}: fused vs layer path, Gaussian3D row {row}"
+        # compositing backward vs the reference, over the splats that lie only
+        # in tiles the reference ordered as we did
+        touched = np.zeros(n, bool)
+        touched[mine["ids"][bad[tile_of]]] = True
+        sel = ~touched & (mine["counts"] > 0)
+        G2r = R.download(9)
+        for row in SPLAT2D_ROWS:
+            e = rel_err(G2g[row][sel], G2r[row][sel])
+            key = "splat2d_cov_ref" if row in COV_ROWS else "splat2d_ref"
+            worst[key] = max(worst[key], e)
+            assert e <= _tol(row), f"{where}: Splat2D row {row} vs reference"
+        # projection + activation backward of the reference's own Splat2D
+        # gradients reproduce its Gaussian3D gradients
+        S3r = torch.tensor(R.download(10), device="cuda")
+        G3m = api.project_backward(S3r, prob.pv, torch.tensor(G2r, device="cuda"))
+        GPm = api.activ_backward(Pt, S3r, G3m, 0, prob.cam).cpu().numpy()
+        GPr = R.download(6)
+        for row in range(GPr.shape[0]):
+            e = rel_err(GPm[row], GPr[row])
+            worst["g3d_ref"] = max(worst["g3d_ref"], e)
+            assert e <= GRAD_TOL, f"{where}: Gaussian3D row {row} vs reference"
+        if c % ORACLE_EVERY == 0:
+            S2f = S2g.cpu().numpy().astype(np.float64)
+            cxx, cxy, cyy = S2f[3], S2f[4], S2f[5]
+            ill = cxx * cyy - cxy * cxy < 1e-2 * np.abs(cxx * cyy)
+            ill_max = max(ill_max, int((ill & (mine["counts"] > 0)).sum()))
+            # The oracle's forward gets the covariance whose FP64 inverse is
+            # the FP32 conic our compositing (like the reference's) evaluates:
+            # the FP32 1 / det of a nearly singular covariance is off from the
+            # FP64 one by more than the tolerances.
+            con = f.download(L.DS_RASTER_CONICS).reshape(n, 4).astype(np.float64)
+            S2c = S2f.copy()
+            vis_all = mine["counts"] > 0
+            a, b, cc = con[vis_all, 0], con[vis_all, 1], con[vis_all, 2]
+            dc = a * cc - b * b
+            S2c[3, vis_all], S2c[4, vis_all], S2c[5, vis_all] = cc / dc, -b / dc, a / dc
+            oimg, _, olast, pamb = O.composite_forward(S2c, W, H, mine["ids"], mine["ranges"],
+                                                       tol=1e-4)
+            good = pamb == 0
+            assert good.mean() > 0.98, where
+            # The FP32 quadratic form of a very elongated splat (det < 1e-3
+            # cxx cyy) cancels, here as in the reference (:277-281), by more
+            # than the threshold tolerance; where such a splat decides it, a
+            # pixel may end on a neighbouring last contributor (one or two
+            # pixels a frame).  Those pixels are left out of the image check.
+            very_ill = cxx * cyy - cxy * cxy < 1e-3 * np.abs(cxx * cyy)
+            flips = np.argwhere(good & (mine["last_ids"] != olast))
+            ntx = (W + 15) // 16
+            for y, x in flips:
+                t = (y // 16) * ntx + x // 16
+                hi = max(mine["last_ids"][y, x], olast[y, x])
+                assert very_ill[mine["ids"][mine["ranges"][2 * t]:hi + 1]].any(), \
+                    f"{where}: last contributor of pixel {(y, x)}"
+                good[y, x] = False
+            flips_max = max(flips_max, len(flips))
+            e = rel_err(mine["image"][good], oimg[good])
+            worst["img_fp64"] = max(worst["img_fp64"], e)
+            assert e <= IMG_TOL, f"{where}: image vs FP64 oracle"
+            alphas = f.download(L.DS_RASTER_ALPHAS).reshape(H, W)
+            gimg = 2.0 / (W * H) * (mine["image"].astype(np.float64) - prob.target)
+            G2o = O.composite_backward(S2f, W, H, mine["ids"], mine["ranges"], alphas,
+                                       mine["last_ids"], gimg)
+            vis = (mine["counts"] > 0) & ~ill
+            both = vis & sel
+            for row in SPLAT2D_ROWS:
+                e = rel_err(G2g[row][vis], G2o[row][vis])
+                key = "splat2d_cov_fp64" if row in COV_ROWS else "splat2d_fp64"
+                worst[key] = max(worst[key], e)
+                assert e <= _tol(row), f"{where}: Splat2D row {row} vs FP64 oracle"
+                if row in COV_ROWS:
+                    # the reference's own FP32 against FP64, same splats
+                    worst["splat2d_cov_ref_fp64"] = max(
+                        worst["splat2d_cov_ref_fp64"], rel_err(G2r[row][both], G2o[row][both]))
+                    worst["splat2d_cov_ours_fp64"] = max(
+                        worst["splat2d_cov_ours_fp64"], rel_err(G2g[row][both], G2o[row][both]))
         checked += 1
         f.step(EVERY - 1)
     code, flags = f.status()
     assert code == 0 and flags == 0
     R.close()
+    raster.close()
     f.close()
     assert checked == STEPS // EVERY
-    print(f"{checked} checkpoints over {STEPS} steps; worst image {worst_img:.2e}, "
-          f"worst gradient {worst_grad:.2e}; pixels in tiles of identical order >= "
-          f"{same_frac:.3f}")
+    print(f"{checked} checkpoints over {STEPS} steps; pixels in tiles of our order >= "
+          f"{same_frac:.3f}; worst relative errors: " +
+          ", ".join(f"{k} {v:.2e}" for k, v in worst.items()) +
+          f"; at most {ill_max} visible splats with a nearly singular covariance left out "
+          f"of the FP64 gradient comparison, {flips_max} pixels a frame with a last "
+          f"contributor moved by a very elongated splat")
