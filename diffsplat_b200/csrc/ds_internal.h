@@ -91,6 +91,9 @@ int launch_project_backward(const ds_splat3d& in, const float pv[16], const ds_s
 // captured into a CUDA graph.  Fixed grid of kSortBlocks CTAs.
 // ---------------------------------------------------------------------------
 constexpr int kSortBlocks = 296;    // 2 x 148 SMs
+// Tile grids up to this size sort their pairs by a single stable counting
+// pass (ds_raster.cu); larger ones by radix passes over the tile id.
+constexpr int kCountSortMaxTiles = 8192;
 constexpr int kSortTileItems = 2048;  // items per CTA iteration (8 warps x 32 lanes x 8)
 
 struct SortScratch {
@@ -141,7 +144,7 @@ struct DevScalars {
   uint32_t n_splats;  // element count of the depth sort
   uint32_t step;      // Adam step count (fitter)
   uint32_t n_long;    // splats with more than kSerialRecords tiles (last emission scan)
-  uint32_t pad;
+  uint32_t sort_ticket;  // CTA-completion counter of the tile-offset scan
   unsigned long long n_isects_raw;  // unclamped pair count
   float loss;
   float pad2;
@@ -207,6 +210,13 @@ struct RasterBuffers {
   uint32_t* sorted_emit = nullptr;
   uint32_t* depth_perm = nullptr;         // depth-sorted splat ids
   uint32_t* depth_sorted_keys = nullptr;  // their depth keys
+
+  // Counting sort of the pairs by tile (grids of at most kCountSortMaxTiles
+  // tiles; null: the radix path): per-chunk tile counts, then their column
+  // prefix [count_chunks][tiles], and the per-tile totals.
+  uint32_t* tile_hist = nullptr;
+  uint32_t* tile_totals = nullptr;
+  int count_chunks = 0;
 
   // per tile / pixel
   int2* ranges = nullptr;

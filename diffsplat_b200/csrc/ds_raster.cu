@@ -15,6 +15,8 @@
 //     record per (tile, splat) pair and a warp per splat sums each splat's
 //     records here: no global atomics, deterministic gradients.
 #include <float.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <vector>
@@ -275,6 +277,216 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---- stable counting sort of the pairs by tile --------------------------------
+// The emission lays the pairs out grouped by splat in (depth, id) order; a
+// stable partition by tile id gives each tile's list in that order, which is
+// the reference's 64-bit (tile | depth) key order with equal keys by id.
+// The n pairs are split into count_chunks contiguous chunks (one CTA each,
+// split again into contiguous warp runs):
+//   tile_count_kernel   per chunk, pairs per tile -> hist[chunk][tile]
+//   tile_offsets_kernel per tile, exclusive prefix of hist over the chunks
+//                       (in place) and the total; the last CTA to finish
+//                       scans the totals into the tile ranges
+//   tile_scatter_kernel per chunk, each warp ranks its run in order (match
+//                       over the lanes' tile ids) and writes every pair to
+//                       range start + chunk prefix + warp prefix + rank.
+// One pass over the pairs instead of ceil(log2 T / 8) radix passes, and the
+// ranges come out of the scan.
+constexpr int kOffsetThreads = 1024;  // 32 tiles x 32 slices of the chunk column
+
+__device__ __forceinline__ void chunk_of(uint32_t n, uint32_t chunks, uint32_t c, uint32_t& lo,
+                                         uint32_t& hi) {
+  const uint32_t per = (n + chunks - 1) / chunks;
+  lo = min(n, c * per);
+  hi = min(n, lo + per);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    tile_count_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ n_dev,
+                      int tiles, uint32_t* __restrict__ hist, uint32_t* __restrict__ status) {
+  pdl_wait();
+  extern __shared__ uint32_t cnt[];  // [tiles]
+  for (int t = threadIdx.x; t < tiles; t += kThreads) cnt[t] = 0u;
+  __syncthreads();
+  uint32_t lo, hi;
+  chunk_of(*n_dev, gridDim.x, blockIdx.x, lo, hi);
+  constexpr int kAhead = 4;
+  for (uint32_t e0 = lo + threadIdx.x; e0 < hi; e0 += kThreads * kAhead) {
+    uint32_t tk[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const uint32_t e = e0 + u * kThreads;
+      tk[u] = e < hi ? tile_keys[e] : 0xfffffffeu;
+    }
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      if (tk[u] < (uint32_t)tiles) atomicAdd(&cnt[tk[u]], 1u);
+      else if (tk[u] != 0xfffffffeu) atomicOr(status, kStatusBadTile);  // never when correct
+    }
+  }
+  __syncthreads();
+  uint32_t* row = hist + (size_t)blockIdx.x * tiles;
+  for (int t = threadIdx.x; t < tiles; t += kThreads) row[t] = cnt[t];
+}
+
+__global__ void __launch_bounds__(kOffsetThreads)
+    tile_offsets_kernel(uint32_t* __restrict__ hist, int chunks, int tiles,
+                        uint32_t* __restrict__ totals, int2* __restrict__ ranges,
+                        DevScalars* __restrict__ sc) {
+  pdl_wait();
+  constexpr int kSlices = kOffsetThreads / 32;
+  __shared__ uint32_t part[kSlices][33];
+  __shared__ uint32_t wsum[kSlices];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+  const int t = blockIdx.x * 32 + lane;
+  const int r0 = s * chunks / kSlices, r1 = (s + 1) * chunks / kSlices;
+  uint32_t sum = 0;
+  if (t < tiles) {
+#pragma unroll 4
+    for (int r = r0; r < r1; ++r) sum += hist[(size_t)r * tiles + t];
+  }
+  part[s][lane] = sum;
+  __syncthreads();
+  uint32_t run = 0;
+  for (int k = 0; k < s; ++k) run += part[k][lane];
+  if (t < tiles) {
+    for (int r = r0; r < r1; ++r) {
+      const size_t q = (size_t)r * tiles + t;
+      const uint32_t v = hist[q];
+      hist[q] = run;
+      run += v;
+    }
+    if (s == kSlices - 1) totals[t] = run;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&sc->sort_ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // Last CTA: exclusive scan of the totals into the ranges; each thread takes
+  // a contiguous run of tiles.
+  const int per = (tiles + kOffsetThreads - 1) / kOffsetThreads;
+  const int a = min(tiles, threadIdx.x * per), b = min(tiles, a + per);
+  uint32_t mine = 0;
+  for (int k = a; k < b; ++k) mine += ((volatile uint32_t*)totals)[k];
+  uint32_t incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) wsum[s] = incl;
+  __syncthreads();
+  if (s == 0) {
+    const uint32_t w = wsum[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += v;
+    }
+    wsum[lane] = wi - w;  // exclusive over the warps
+  }
+  __syncthreads();
+  uint32_t base = incl - mine + wsum[s];
+  for (int k = a; k < b; ++k) {
+    const uint32_t c = ((volatile uint32_t*)totals)[k];
+    ranges[k] = c ? make_int2((int)base, (int)(base + c)) : make_int2(0, 0);
+    base += c;
+  }
+  if (threadIdx.x == 0) sc->sort_ticket = 0u;
+}
+
+// blockDim.x = 32 * warps; dynamic shared memory (1 + warps) * tiles * 4 B.
+__global__ void __launch_bounds__(kThreads)
+    tile_scatter_kernel(const uint32_t* __restrict__ tile_keys,
+                        const uint32_t* __restrict__ emit_splat, const uint32_t* __restrict__ n_dev,
+                        int tiles, const uint32_t* __restrict__ hist,
+                        const int2* __restrict__ ranges, uint32_t* __restrict__ sorted_splat,
+                        uint32_t* __restrict__ sorted_emit) {
+  pdl_wait();
+  extern __shared__ uint32_t smem[];
+  const int warps = blockDim.x >> 5;
+  uint32_t* base = smem;          // [tiles]: range start + chunk prefix
+  uint32_t* woff = smem + tiles;  // [warps][tiles]: warp counts, then warp prefixes
+  uint32_t lo, hi;
+  chunk_of(*n_dev, gridDim.x, blockIdx.x, lo, hi);
+  if (lo >= hi) return;  // uniform
+  const uint32_t* prefix = hist + (size_t)blockIdx.x * tiles;
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) base[t] = (uint32_t)ranges[t].x + prefix[t];
+  for (int q = threadIdx.x; q < warps * tiles; q += blockDim.x) woff[q] = 0u;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t per = (hi - lo + warps - 1) / warps;
+  const uint32_t wlo = min(hi, lo + w * per), whi = min(hi, wlo + per);
+  uint32_t* mine = woff + (size_t)w * tiles;
+  const uint32_t lt = (1u << lane) - 1u;
+  // The run is walked kAhead warp-steps at a time with all their loads issued
+  // first: the steps depend on one another only through the shared counters.
+  constexpr int kAhead = 8;
+  // 1) pairs per tile in this warp's run
+  for (uint32_t e0 = wlo; e0 < whi; e0 += 32 * kAhead) {
+    uint32_t tk[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const uint32_t e = e0 + 32 * u + lane;
+      tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
+    }
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const uint32_t t = tk[u];
+      const uint32_t peers = __match_any_sync(0xffffffffu, t);
+      if (t < (uint32_t)tiles && (peers & lt) == 0u) mine[t] += (uint32_t)__popc(peers);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // 2) exclusive prefix over the warps, per tile
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+    uint32_t run = 0;
+    for (int k = 0; k < warps; ++k) {
+      const uint32_t c = woff[(size_t)k * tiles + t];
+      woff[(size_t)k * tiles + t] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  // 3) each pair to its slot, in order
+  for (uint32_t e0 = wlo; e0 < whi; e0 += 32 * kAhead) {
+    uint32_t tk[kAhead], sp[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const uint32_t e = e0 + 32 * u + lane;
+      tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
+      sp[u] = e < whi ? emit_splat[e] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const uint32_t t = tk[u];
+      const uint32_t peers = __match_any_sync(0xffffffffu, t);
+      const int leader = __ffs(peers) - 1;
+      const bool valid = t < (uint32_t)tiles;  // false past the run's end
+      uint32_t p0 = 0;
+      if (valid && lane == leader) {
+        p0 = base[t] + mine[t];
+        mine[t] += (uint32_t)__popc(peers);
+      }
+      p0 = __shfl_sync(0xffffffffu, p0, leader);
+      if (valid) {
+        const uint32_t pos = p0 + __popc(peers & lt);
+        sorted_splat[pos] = sp[u];
+        sorted_emit[pos] = e0 + 32 * u + lane;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Warps per scatter CTA: as many as keep three CTAs per SM within 227 KB.
+inline int scatter_warps(int tiles) { return tiles <= 2048 ? 8 : (tiles <= 4096 ? 4 : 2); }
+
 // Longest-first schedule of the composite CTAs: tiles bucketed by their list
 // length (quarter-octave buckets), buckets in descending order.  The heaviest
 // tiles start in the first wave, so they no longer set the kernel's tail.  The
@@ -402,6 +614,34 @@ static int raster_alloc_splats(RasterBuffers& rb, int max_splats, int64_t cap) {
   return DS_OK;
 }
 
+// Scratch of the counting sort for a grid of rb.tiles tiles (none beyond
+// kCountSortMaxTiles, or with DS_TILE_SORT=radix: the radix path then runs).
+static int alloc_count_sort(RasterBuffers& rb) {
+  release(rb.tile_hist);
+  release(rb.tile_totals);
+  rb.count_chunks = 0;
+  static const bool radix_only = [] {
+    const char* e = getenv("DS_TILE_SORT");
+    return e && strcmp(e, "radix") == 0;
+  }();
+  if (radix_only || rb.tiles <= 0 || rb.tiles > kCountSortMaxTiles) return DS_OK;
+  // one chunk per 2 x 148 SMs, at least 512 pairs each
+  rb.count_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(kSortBlocks, (rb.cap + 511) / 512));
+  DS_TRY(alloc(&rb.tile_hist, (size_t)rb.count_chunks * rb.tiles));
+  DS_TRY(alloc(&rb.tile_totals, (size_t)rb.tiles));
+  // the scatter's shared memory (up to 160 KB) is opted into once per device
+  static uint64_t smem_set = 0;
+  int dev = 0;
+  DS_CUDA(cudaGetDevice(&dev));
+  if (dev >= 64 || !(smem_set >> dev & 1u)) {
+    const int most = kCountSortMaxTiles * 4 * (1 + scatter_warps(kCountSortMaxTiles));
+    DS_CUDA(cudaFuncSetAttribute(tile_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 most));
+    if (dev < 64) smem_set |= 1ull << dev;
+  }
+  return DS_OK;
+}
+
 int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap) {
   if (width <= 0 || height <= 0 || max_splats < 0) return DS_ERR_ARG;
   DS_TRY(raster_alloc_splats(rb, max_splats, cap));
@@ -425,7 +665,7 @@ int raster_alloc_batch(RasterBuffers& rb, int64_t pixels, int tiles, int tile_si
   DS_TRY(alloc(&rb.last_ids, (size_t)pixels));
   DS_TRY(alloc(&rb.loss_partials, (size_t)tiles));
   DS_CUDA(cudaMemset(rb.ranges, 0, tiles * sizeof(int2)));
-  return DS_OK;
+  return alloc_count_sort(rb);
 }
 
 int raster_resize(RasterBuffers& rb, int width, int height) {
@@ -449,7 +689,7 @@ int raster_resize(RasterBuffers& rb, int width, int height) {
   DS_TRY(alloc(&rb.last_ids, px));
   DS_TRY(alloc(&rb.loss_partials, (size_t)rb.tiles));
   DS_CUDA(cudaMemset(rb.ranges, 0, rb.tiles * sizeof(int2)));
-  return DS_OK;
+  return alloc_count_sort(rb);
 }
 
 void raster_free(RasterBuffers& rb) {
@@ -484,6 +724,8 @@ void raster_free(RasterBuffers& rb) {
   release(rb.alphas);
   release(rb.last_ids);
   release(rb.loss_partials);
+  release(rb.tile_hist);
+  release(rb.tile_totals);
   rb.width = rb.height = 0;
 }
 
@@ -517,6 +759,26 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
                        n, rb.ntx, (uint32_t)rb.cap, rb.tile_k0, rb.emit_splat, rb.seg_start,
                        rb.inst_of_splat, rb.geom, rb.ranges, rb.tiles));
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
+    if (rb.tile_hist) {
+      // 4) stable counting sort by tile id; the ranges come out of its scan
+      const int T = rb.tiles, G = rb.count_chunks, W = scatter_warps(T);
+      const size_t cnt_smem = (size_t)T * 4;
+      const size_t sct_smem = (size_t)T * 4 * (1 + W);
+      DS_CUDA(launch_pdl(tile_count_kernel, dim3(G), dim3(kThreads), cnt_smem, s, rb.tile_k0,
+                         &sc->n_isects, T, rb.tile_hist, &sc->status));
+      DS_CUDA(launch_pdl(tile_offsets_kernel, dim3((T + 31) / 32), dim3(kOffsetThreads), 0, s,
+                         rb.tile_hist, G, T, rb.tile_totals, rb.ranges, sc));
+      DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * W), sct_smem, s, rb.tile_k0,
+                         rb.emit_splat, &sc->n_isects, T, rb.tile_hist, rb.ranges,
+                         rb.sorted_splat, rb.tile_v0));
+      rb.sorted_emit = rb.tile_v0;
+      rb.sorted_tile = nullptr;
+      if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST)
+        DS_CUDA(launch_pdl(tile_order_kernel, dim3(1), dim3(1024), 0, s, rb.ranges, rb.tiles,
+                           rb.tile_order));
+      if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
+      return cuda_status(cudaGetLastError());
+    }
     // 4) stable sort by tile id; last pass gathers the splat id of each pair
     DS_TRY(radix_sort_pairs(rb.tile_k0, nullptr, rb.tile_k1, rb.tile_v1, rb.tile_k0, rb.tile_v0,
                             &rb.sorted_tile, &rb.sorted_emit, &sc->n_isects, (uint32_t)rb.cap,
@@ -560,14 +822,18 @@ int raster_download(const RasterBuffers& rb, int n_splats, int what, void* host,
       // (tile id << 32) | depth bits of the pair's splat, in sorted order
       if ((size_t)bytes < (size_t)n * 8) return DS_ERR_ARG;
       if (n == 0) return DS_OK;
-      std::vector<uint32_t> tiles(n), ids(n), depth(n_splats > 0 ? n_splats : 1);
-      DS_CUDA(cudaMemcpy(tiles.data(), rb.sorted_tile, (size_t)n * 4, cudaMemcpyDeviceToHost));
+      // the tile of each sorted pair, from the tile ranges
+      std::vector<uint32_t> tiles(n, 0xffffffffu), ids(n), depth(n_splats > 0 ? n_splats : 1);
+      std::vector<int2> rg(rb.tiles > 0 ? rb.tiles : 1);
+      DS_CUDA(cudaMemcpy(rg.data(), rb.ranges, (size_t)rb.tiles * 8, cudaMemcpyDeviceToHost));
+      for (int t = 0; t < rb.tiles; ++t)
+        for (int q = std::max(rg[t].x, 0); q < rg[t].y && q < (int64_t)n; ++q) tiles[q] = (uint32_t)t;
       DS_CUDA(cudaMemcpy(ids.data(), rb.sorted_splat, (size_t)n * 4, cudaMemcpyDeviceToHost));
       DS_CUDA(cudaMemcpy(depth.data(), rb.depth_keys, (size_t)n_splats * 4,
                          cudaMemcpyDeviceToHost));
       uint64_t* k = (uint64_t*)host;
       for (uint32_t q = 0; q < n; ++q) {
-        if (ids[q] >= (uint32_t)n_splats) return DS_ERR_INTERNAL;
+        if (ids[q] >= (uint32_t)n_splats || tiles[q] == 0xffffffffu) return DS_ERR_INTERNAL;
         k[q] = ((uint64_t)tiles[q] << 32) | depth[ids[q]];
       }
       return DS_OK;
