@@ -399,7 +399,9 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                          const float* __restrict__ grad_or_image, const float* __restrict__ target,
                          float* __restrict__ isect_grad, int W_, int H_, int ntx_,
                          const uint16_t* __restrict__ tile_inst,
-                         const InstGeom* __restrict__ geom) {
+                         const InstGeom* __restrict__ geom,
+                         const uint32_t* __restrict__ depth_keys,
+                         unsigned long long* __restrict__ tile_bound) {
   pdl_wait();
   using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
@@ -410,10 +412,14 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   __shared__ uint32_t sMask[B];
   __shared__ float4 sBox[NW];
   __shared__ __align__(16) float part[NW][B * 9];  // per-warp partial of each batch splat
+  __shared__ int32_t sFinal[NW];
   const int tile = order ? order[blockIdx.x] : (int)blockIdx.x;
   const int2 range = ranges[tile];
-  const int start = range.x, end = range.y;
-  if (end <= start) return;
+  const int start = range.x;
+  if (range.y <= start) {
+    if (threadIdx.x == 0) tile_bound[tile] = 0ull;
+    return;
+  }
   const TileGeo tg = tile_geo<kBatch>(tile, W_, H_, ntx_, tile_inst, geom);
   const int W = tg.W, H = tg.H;
   const Pixels<PPT> m = pixels<PPT, TS>(tg.local, tg.ntx, W, H);
@@ -445,6 +451,24 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     acc[k] = 0.f;
   }
   const int32_t warp_final = warp_max(my_final);
+  // Pairs after the tile's last contributing splat reach no pixel: the list
+  // ends there for the backward, and no record is written for them (their
+  // consumers skip them by tile_bound).
+  if (lane == 0) sFinal[w] = warp_final;
+  __syncthreads();
+  int32_t tile_final = sFinal[0];
+#pragma unroll
+  for (int k = 1; k < NW; ++k) tile_final = max(tile_final, sFinal[k]);
+  const int end = min(range.y, tile_final + 1);
+  if (threadIdx.x == 0) {
+    unsigned long long bound = 0ull;
+    if (end > start) {
+      const uint32_t last = sorted_splat[end - 1];
+      bound = (((unsigned long long)depth_keys[last] << 32) | last) + 1ull;
+    }
+    tile_bound[tile] = bound;
+  }
+  if (end <= start) return;
   const int nb = (end - start + B - 1) / B;
   // Threads per staged splat: with twice as many threads as batch slots, two
   // threads share a splat's warp-block tests and its cross-warp sum.
@@ -665,7 +689,7 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
   launch_pdl(composite_bwd_kernel<PPT, TS, F, E, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
              rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit,      \
              rb.ranges, order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width,         \
-             rb.height, rb.ntx, rb.tile_inst, rb.geom)
+             rb.height, rb.ntx, rb.tile_inst, rb.geom, rb.depth_keys, rb.tile_bound)
   if (grad_rgb) {
     if (exact) DS_BWD(false, true);
     else DS_BWD(false, false);

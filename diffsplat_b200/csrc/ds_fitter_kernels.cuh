@@ -183,10 +183,26 @@ __global__ void __launch_bounds__(kThreads)
     } else {
 #pragma unroll
       for (int k = 0; k < 9; ++k) g2[k] = 0.f;
-      for (unsigned long long q = s0; q < e0; ++q) {
-        const float* r = seg.rec + q * 9;
+      if (e0 > s0) {
+        // records of the tiles whose list ends (for compositing) before this
+        // splat were not written: skip them
+        const ushort4 rc = seg.rect[i];
+        const uint32_t w = (uint32_t)(rc.y - rc.x + 1);
+        uint32_t row0, pitch;
+        seg_origin(seg, (uint32_t)i, rc, row0, pitch);
+        const unsigned long long key = seg_key(seg, (uint32_t)i);
+        uint32_t tx = 0, trow = row0;
+        for (unsigned long long q = s0; q < e0; ++q) {
+          if (key < seg.tile_bound[trow + tx]) {
+            const float* r = seg.rec + q * 9;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) g2[k] += r[k];
+            for (int k = 0; k < 9; ++k) g2[k] += r[k];
+          }
+          if (++tx == w) {
+            tx = 0;
+            trow += pitch;
+          }
+        }
       }
     }
   }

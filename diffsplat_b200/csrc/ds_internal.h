@@ -219,6 +219,7 @@ struct RasterBuffers {
   int count_chunks = 0;
 
   // per tile / pixel
+  unsigned long long* tile_bound = nullptr;  // see GradSegments
   int2* ranges = nullptr;
   int32_t* tile_order = nullptr;  // composite schedule: tiles by descending list length
   float* alphas = nullptr;
@@ -232,16 +233,46 @@ struct RasterBuffers {
 };
 
 // Where a consumer finds splat i's gradient records: [start[i], start[i] +
-// counts[i]) clamped to cap, 9 floats each.
+// counts[i]) clamped to cap, 9 floats each, record k for the k-th tile of the
+// splat's rectangle in row-major order.  The composite backward writes no
+// record for a pair that lies in its tile's list after the tile's last
+// contributing splat (nothing reaches a pixel from there); tile_bound[t] is 1 +
+// the (depth key << 32 | splat id) of that last splat, 0 when none: record k
+// counts only when the splat's key is below the bound of its tile.
 struct GradSegments {
   const float* rec;
   const uint32_t* counts;
   const uint32_t* start;
   uint32_t cap;
+  const unsigned long long* tile_bound;
+  const uint32_t* depth_keys;
+  const ushort4* rect;
+  int ntx;
+  const uint16_t* inst_of_splat;  // batches: tile ids are batch-wide
+  const InstGeom* geom;
 };
 inline GradSegments grad_segments(const RasterBuffers& rb) {
-  return GradSegments{rb.isect_grad, rb.counts, rb.seg_start, (uint32_t)rb.cap};
+  return GradSegments{rb.isect_grad, rb.counts, rb.seg_start, (uint32_t)rb.cap, rb.tile_bound,
+                      rb.depth_keys, rb.rect, rb.ntx, rb.inst_of_splat, rb.geom};
 }
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned long long seg_key(const GradSegments& g, uint32_t i) {
+  return ((unsigned long long)g.depth_keys[i] << 32) | i;
+}
+// First tile id of the splat's rectangle and its row pitch.
+__device__ __forceinline__ void seg_origin(const GradSegments& g, uint32_t i, const ushort4& r,
+                                           uint32_t& row0, uint32_t& pitch) {
+  uint32_t base = 0;
+  pitch = (uint32_t)g.ntx;
+  if (g.geom) {
+    const InstGeom gg = g.geom[g.inst_of_splat[i]];
+    base = (uint32_t)gg.tile_off;
+    pitch = (uint32_t)gg.ntx;
+  }
+  row0 = base + (uint32_t)r.z * pitch + r.x;
+}
+#endif
 
 int raster_alloc(RasterBuffers& rb, int width, int height, int max_splats, int64_t cap);
 // Pixels per thread of the composite kernels; DS_COMPOSITE_PPT=1|2|4 overrides

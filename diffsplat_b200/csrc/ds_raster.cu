@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kThreads)
                                 const uint32_t* __restrict__ perm,
                                 const unsigned long long* __restrict__ offsets,
                                 const uint32_t* __restrict__ counts, uint32_t cap, int n,
-                                float* __restrict__ g2, ds_splat2d gin) {
+                                float* __restrict__ g2, ds_splat2d gin, GradSegments seg) {
   const int p = (int)(blockIdx.x * (int64_t)kThreads + threadIdx.x);
   if (p >= n) return;
   uint32_t i, c;
@@ -210,10 +210,24 @@ __global__ void __launch_bounds__(kThreads)
   segment_of(perm, offsets, counts, cap, p, i, c, s, e);
   if (c > kSerialRecords || (kAccumulate && c == 0)) return;
   float v[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  for (unsigned long long q = s; q < e; ++q) {
-    const float* r = isect_grad + q * 9;
+  if (e > s) {
+    const ushort4 rc = seg.rect[i];
+    const uint32_t w = (uint32_t)(rc.y - rc.x + 1);
+    uint32_t row0, pitch;
+    seg_origin(seg, i, rc, row0, pitch);
+    const unsigned long long key = seg_key(seg, i);
+    uint32_t tx = 0, trow = row0;
+    for (unsigned long long q = s; q < e; ++q) {
+      if (key < seg.tile_bound[trow + tx]) {
+        const float* r = isect_grad + q * 9;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) v[k] += r[k];
+        for (int k = 0; k < 9; ++k) v[k] += r[k];
+      }
+      if (++tx == w) {
+        tx = 0;
+        trow += pitch;
+      }
+    }
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) store_g2<kAccumulate>(k, i, n, v[k], g2, gin);
@@ -224,7 +238,7 @@ __global__ void __launch_bounds__(kThreads)
     segment_reduce_long_kernel(const float* __restrict__ isect_grad, int n,
                                float* __restrict__ g2, ds_splat2d gin,
                                const uint4* __restrict__ long_list,
-                               DevScalars* __restrict__ sc) {
+                               DevScalars* __restrict__ sc, GradSegments sg) {
   pdl_wait();
   const int lane = threadIdx.x & 31;
   const uint32_t total = sc->n_long;
@@ -235,11 +249,34 @@ __global__ void __launch_bounds__(kThreads)
     const unsigned long long s = seg.y, e = seg.z;
     float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float a = 0.f;
+    const ushort4 rc = sg.rect[i];
+    const uint32_t wd = (uint32_t)(rc.y - rc.x + 1);
+    uint32_t row0, pitch;
+    seg_origin(sg, i, rc, row0, pitch);
+    const unsigned long long key = seg_key(sg, i);
+    // record q is tile k = q - first of the row-major rectangle; lanes step by
+    // 32 = 32 / wd rows and 32 % wd columns
+    const uint32_t first = sg.start[i];
+    uint32_t ty = 0, tx = 0;
+    if (s + lane < e) {
+      const uint32_t k = (uint32_t)(s + lane - first);
+      ty = k / wd;
+      tx = k - ty * wd;
+    }
+    const uint32_t dy = 32u / wd, dx = 32u - dy * wd;
     for (unsigned long long q = s + lane; q < e; q += 32) {
-      const float* r = isect_grad + q * 9;
+      if (key < sg.tile_bound[row0 + ty * pitch + tx]) {
+        const float* r = isect_grad + q * 9;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] += r[k];
-      a += r[8];
+        for (int k = 0; k < 8; ++k) v[k] += r[k];
+        a += r[8];
+      }
+      ty += dy;
+      tx += dx;
+      if (tx >= wd) {
+        tx -= wd;
+        ++ty;
+      }
     }
     const float s8 = warp_sum8_transposed(v, lane);
     const float sa = warp_sum(a);
@@ -254,7 +291,7 @@ int launch_long_reduce(RasterBuffers& rb, int n, const ds_splat2d& gin, cudaStre
   const int64_t warps = std::min<int64_t>(n, kLongWarps);
   const unsigned blocks = (unsigned)((warps * 32 + kThreads - 1) / kThreads);
   DS_CUDA(launch_pdl(segment_reduce_long_kernel<kAccumulate>, dim3(blocks), dim3(kThreads), 0, s,
-                     rb.isect_grad, n, rb.g2, gin, rb.long_list, rb.scalars));
+                     rb.isect_grad, n, rb.g2, gin, rb.long_list, rb.scalars, grad_segments(rb)));
   return cuda_status(cudaGetLastError());
 }
 
@@ -660,6 +697,7 @@ int raster_alloc_batch(RasterBuffers& rb, int64_t pixels, int tiles, int tile_si
   rb.nty = 1;
   rb.tiles = tiles;
   DS_TRY(alloc(&rb.ranges, (size_t)tiles));
+  DS_TRY(alloc(&rb.tile_bound, (size_t)tiles));
   DS_TRY(alloc(&rb.tile_order, (size_t)tiles));
   DS_TRY(alloc(&rb.alphas, (size_t)pixels));
   DS_TRY(alloc(&rb.last_ids, (size_t)pixels));
@@ -672,6 +710,7 @@ int raster_resize(RasterBuffers& rb, int width, int height) {
   if (width <= 0 || height <= 0) return DS_ERR_ARG;
   if (width == rb.width && height == rb.height) return DS_OK;
   release(rb.ranges);
+  release(rb.tile_bound);
   release(rb.tile_order);
   release(rb.alphas);
   release(rb.last_ids);
@@ -684,6 +723,7 @@ int raster_resize(RasterBuffers& rb, int width, int height) {
   if (rb.ntx > 65535 || rb.nty > 65535) return DS_ERR_ARG;
   const size_t px = (size_t)width * height;
   DS_TRY(alloc(&rb.ranges, (size_t)rb.tiles));
+  DS_TRY(alloc(&rb.tile_bound, (size_t)rb.tiles));
   DS_TRY(alloc(&rb.tile_order, (size_t)rb.tiles));
   DS_TRY(alloc(&rb.alphas, px));
   DS_TRY(alloc(&rb.last_ids, px));
@@ -720,6 +760,7 @@ void raster_free(RasterBuffers& rb) {
   release(rb.scan.long_partials);
   release(rb.scalars);
   release(rb.ranges);
+  release(rb.tile_bound);
   release(rb.tile_order);
   release(rb.alphas);
   release(rb.last_ids);
@@ -873,7 +914,8 @@ int raster_reduce_grads(RasterBuffers& rb, const ds_splat2d& gin, int n, cudaStr
   if (n <= 0) return DS_OK;
   segment_reduce_short_kernel<true><<<(unsigned)(((int64_t)n + kThreads - 1) / kThreads), kThreads,
                                       0, s>>>(rb.isect_grad, rb.depth_perm, rb.emit_offsets,
-                                              rb.counts, (uint32_t)rb.cap, n, rb.g2, gin);
+                                              rb.counts, (uint32_t)rb.cap, n, rb.g2, gin,
+                                              grad_segments(rb));
   DS_CUDA(cudaGetLastError());
   return launch_long_reduce<true>(rb, n, gin, s);
 }
