@@ -138,25 +138,44 @@ NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.42176e6 / 3085768,
 
 
 def kernels_per_step(tiles: int) -> int:
-    passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
-    # step_begin, preprocess, 4 depth passes x 3, scan x 2, emit, tile passes x 3,
-    # ranges, tile schedule, composite fwd, composite bwd, long-segment reduce,
-    # backward+Adam (which sums the short segments itself)
-    return 2 + 12 + 2 + 1 + 3 * passes + 2 + 4
+    # step_begin, preprocess, 4 depth-sort passes x 3, count scan x 2, emission,
+    # tile sort (grids of up to 8192 tiles: count, offsets + ranges, scatter;
+    # larger: 3 kernels per radix pass over the tile id, then ranges), tile
+    # schedule, composite forward, composite backward (two launches, one per
+    # pixel layout, each taking its own tiles), long-segment reduce,
+    # backward + Adam (which sums the short segments itself)
+    if tiles <= 8192:
+        tile_sort = 3
+    else:
+        tile_sort = 3 * max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8) + 1
+    return 2 + 12 + 2 + 1 + tile_sort + 1 + 1 + 2 + 2
 
 
-def stage_bytes(n: int, isects: int, pixels: int, tiles: int) -> dict:
-    """Algorithmic HBM bytes per launch of each stage (FP32 storage, SH 0)."""
-    passes = max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8)
+def stage_bytes(n: int, isects: int, pixels: int, bands: int = 0) -> dict:
+    """Algorithmic HBM bytes per step of each stage group, by the per-unit
+    figures of the path's measurement plan (FP32 storage):
+      activation + projection  (14 + 3K) * 4 B read + 40 B written per splat
+      tile assign              24 B read per splat + 12 B written per pair
+      sort                     24 B per pair (the single-pass lower bound)
+      ranges                   8 B per pair
+      composite forward        40 B per pair + 20 B per pixel
+      composite backward       44 B per pair + 20 B per pixel
+      Adam                     28 B per parameter element (p, g, m, v)."""
+    elems = 14 + 3 * bands
     return {
-        "preprocess": n * (14 * 4 + 48 + 4 + 8 + 4 + 4),
-        "depth_sort": 4 * n * 16,
-        "scan_emit": n * 16 + isects * 8,
-        "tile_sort_ranges": passes * isects * 16 + isects * 8,
-        "composite_fwd": isects * (4 + 48) + pixels * (12 + 12 + 4 + 4),
-        "composite_bwd": isects * (4 + 4 + 52 + 36) + pixels * (12 + 12 + 4 + 4),
-        "backward_adam": n * (14 * 4 * 6) + isects * 36,
+        "preprocess": n * (elems * 4 + 40),
+        "lists": n * 24 + isects * (12 + 24 + 8),
+        "composite_fwd": isects * 40 + pixels * 20,
+        "composite_bwd": isects * 44 + pixels * 20,
+        "backward_adam": n * elems * 28,
     }
+
+
+# Stage groups of the fitter's profile step timed against each algorithmic figure.
+STAGE_GROUPS = {"preprocess": ("preprocess",),
+                "lists": ("depth_sort", "scan_emit", "tile_sort_ranges"),
+                "composite_fwd": ("composite_fwd",), "composite_bwd": ("composite_bwd",),
+                "backward_adam": ("backward_adam",)}
 
 
 def cpu_baseline_oracle(prob, budget_s: float = 10.0) -> dict:
@@ -600,7 +619,11 @@ def main():
     config = {"workload": "reference-default fitter: 1280x720 procedural target (2000 blobs), "
                           "60000 splats, SH 0, 16x16 tiles, MSE, Adam (Gaussian3DAdamConfig lrs)",
               "width": 1280, "height": 720, "splats": 60000, "sh_degree": 0,
-              "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"}
+              "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}",
+              "steps_before_timed": args.warmup,
+              "fit_state": f"timed steps {args.warmup + 1}-{args.warmup + args.steps} of the fit "
+                           "from its initial state (the composite's cost falls as the fit "
+                           "proceeds)"}
     line = {"metric": METRIC, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural)",
@@ -635,15 +658,22 @@ def main():
     tiles = ((prob.width + 15) // 16) * ((prob.height + 15) // 16)
     isects = r["counters"]["n_isects"]
     n = prob.params.shape[1]
-    sb = stage_bytes(n, isects, pixels, tiles)
+    sb = stage_bytes(n, isects, pixels, [0, 3, 8, 15][prob.sh_degree])
     stages = r["stages"]
     dom = max(stages, key=stages.get)
     peaks = measured_peaks()
     pairs = r["pairs"]["contributing"]
     fp32_peak = fp32_peak_tflops(r["clocks"].get("sm_max_mhz") or peaks["sm_max_mhz"])
     tflops = {k: pairs * FLOPS_PER_PAIR[k] / (stages[k] * 1e-3) / 1e12 for k in FLOPS_PER_PAIR}
-    gbs = sb[dom] / (stages[dom] * 1e-3) / 1e9
+    dom_bytes = sb.get(dom, 0)
+    gbs = dom_bytes / (stages[dom] * 1e-3) / 1e9
     traffic = NCU_DRAM_BYTES_PER_ISECT.get(dom)
+    stage_hbm = {}
+    for g, parts in STAGE_GROUPS.items():
+        ms = sum(stages[p] for p in parts)
+        a = sb[g] / (ms * 1e-3) / 1e9
+        stage_hbm[g] = {"algorithmic_bytes": sb[g], "ms": ms, "achieved_gbs": a,
+                        "frac": a / peaks["hbm_gbs"]}
     line.update({
         "value": value, "ms_per_step": r["t_ms"] / args.steps,
         "mpix_per_s": value * pixels / 1e6,
@@ -662,7 +692,8 @@ def main():
                      "composite_fwd_tflops": tflops["composite_fwd"],
                      "hbm": {"achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                              "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
-                             "algorithmic_bytes": sb[dom]}},
+                             "algorithmic_bytes": dom_bytes}},
+        "stage_hbm": {"peak_gbs": peaks["hbm_gbs"], "peak_src": peaks["src"], **stage_hbm},
         "stage_ms": stages, "n_isects": isects, "visible": r["counters"]["visible"],
         "final_loss": r["loss"], "status": r["status"],
     })

@@ -366,6 +366,10 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+__device__ __forceinline__ uint32_t warp_sum_u32(uint32_t v) {
+  return __reduce_add_sync(0xffffffffu, v);
+}
+
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));

@@ -46,6 +46,16 @@ constexpr int kBwdGroupPpt1 = DS_BWD_GROUP;  // backward hits evaluated together
 #define DS_BWD_MIN_BLOCKS 4
 #endif
 
+// Backward layout chosen per forward when ppt_bwd is 0: two pixels per thread
+// (8x8-pixel warp blocks, one warp reduction per 64 pixels) when the
+// forward's hits had at least 24.7 contributing pixels of the 32 of an 8x4
+// block on average, one otherwise.  Measured on the 1280x720 / 60000-splat fit
+// at steps 25-4000: the two-pixel backward is faster down to about 24.7 (0.49
+// vs 0.63 ms at 26.6, early in the fit), equal there and slower below (0.64
+// vs 0.48 ms at 21.9, late).  Chosen for a whole frame: a per-tile choice
+// (two launches splitting the tiles) measured slower than either layout alone.
+constexpr uint32_t kDenseLanesX10 = 247;
+
 template <int PPT, int TS>
 struct Lay {
   static constexpr int kThreads = TS * TS / PPT;
@@ -200,12 +210,13 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                          int32_t* __restrict__ last_ids, int W_, int H_, int ntx_,
                          const uint16_t* __restrict__ tile_inst, const InstGeom* __restrict__ geom,
                          const float* __restrict__ target, float* __restrict__ loss_partials,
-                         DevScalars* __restrict__ sc) {
+                         DevScalars* __restrict__ sc, DevScalars* __restrict__ mode_sc) {
   pdl_wait();
   using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
   constexpr int NW = Lc::kWarps;
   __shared__ float4 sA[kFwdBatch], sB[kFwdBatch], sC[kFwdBatch];
+  __shared__ uint32_t sHits[NW], sLanes[NW];
   __shared__ uint32_t sMask[kFwdBatch];
   __shared__ float4 sBox[NW];
   __shared__ float red[NW];
@@ -223,6 +234,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   bool done[PPT];
   bool all_done = true;
   uint32_t n_contrib = 0, n_tested = 0;
+  uint32_t n_hits = 0, n_lanes = 0;  // this warp's hits and their contributing lanes
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     T[k] = 1.f;
@@ -284,6 +296,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
           ng += word ? 1 : 0;
           word &= word - 1u;
         }
+        n_hits += (uint32_t)ng;
         float4 ag[Lc::kFwdGroup], bg[Lc::kFwdGroup], cg[Lc::kFwdGroup];
 #pragma unroll
         for (int g = 0; g < Lc::kFwdGroup; ++g) {
@@ -304,6 +317,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
             if (kCount) ++n_tested;
             if (al[g] > 0.f) {
               if (kCount) ++n_contrib;
+              ++n_lanes;
               const float vis = al[g] * T[k];
               Cr[k] = __fmaf_rn(cg[g].x, vis, Cr[k]);
               Cg[k] = __fmaf_rn(cg[g].y, vis, Cg[k]);
@@ -334,6 +348,35 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     if ((threadIdx.x & 31) == 0) {
       atomicAdd(&sc->pairs[0], (unsigned long long)a);
       atomicAdd(&sc->pairs[1], (unsigned long long)t);
+    }
+  }
+  if (mode_sc) {
+    const uint32_t lanes = warp_sum_u32(n_lanes);
+    if (lane == 0) {
+      sHits[w] = n_hits;
+      sLanes[w] = lanes;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long h = 0, c = 0;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        h += sHits[k];
+        c += sLanes[k];
+      }
+      atomicAdd(&mode_sc->mode_hits, h);
+      atomicAdd(&mode_sc->mode_lanes, c);
+      __threadfence();
+      if (atomicAdd(&mode_sc->mode_ticket, 1u) == gridDim.x - 1) {
+        // the last CTA decides for the frame and clears the sums
+        __threadfence();
+        const unsigned long long th = atomicAdd(&mode_sc->mode_hits, 0ull);
+        const unsigned long long tc = atomicAdd(&mode_sc->mode_lanes, 0ull);
+        mode_sc->bwd_ppt = (th > 0ull && 10ull * tc >= kDenseLanesX10 * th) ? 2u : 1u;
+        mode_sc->mode_hits = 0ull;
+        mode_sc->mode_lanes = 0ull;
+        mode_sc->mode_ticket = 0u;
+      }
     }
   }
   float l = 0.f;
@@ -401,7 +444,8 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
                          const uint16_t* __restrict__ tile_inst,
                          const InstGeom* __restrict__ geom,
                          const uint32_t* __restrict__ depth_keys,
-                         unsigned long long* __restrict__ tile_bound) {
+                         unsigned long long* __restrict__ tile_bound,
+                         const DevScalars* __restrict__ mode_sc) {
   pdl_wait();
   using Lc = Lay<PPT, TS>;
   constexpr int NT = Lc::kThreads;
@@ -414,6 +458,9 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   __shared__ __align__(16) float part[NW][B * 9];  // per-warp partial of each batch splat
   __shared__ int32_t sFinal[NW];
   const int tile = order ? order[blockIdx.x] : (int)blockIdx.x;
+  // ppt_bwd == 0: the forward chose the layout for this frame; the other
+  // layout's launch returns at once
+  if (mode_sc && (PPT == 2) != (mode_sc->bwd_ppt == 2u)) return;
   const int2 range = ranges[tile];
   const int start = range.x;
   if (range.y <= start) {
@@ -661,16 +708,22 @@ const int32_t* schedule(const RasterBuffers& rb) {
   return rb.schedule == DS_SCHEDULE_LONGEST_FIRST ? rb.tile_order : nullptr;
 }
 
+// Whether the forward chooses the backward's layout (see kDenseLanesX10).
+bool adaptive_bwd(const RasterBuffers& rb) {
+  return rb.ppt_bwd == 0 && rb.ppt == 1 && !rb.geom;
+}
+
 template <int PPT, int TS, bool kBatch>
 void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, bool count,
                 cudaStream_t s) {
   constexpr int NT = Lay<PPT, TS>::kThreads;
   const int32_t* order = schedule(rb);
+  DevScalars* mode = (!count && PPT == 1 && adaptive_bwd(rb)) ? rb.scalars : nullptr;
 #define DS_FWD(L, C)                                                                         \
   launch_pdl(composite_fwd_kernel<PPT, TS, L, C, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
              rb.rec_a, rb.rec_b, rb.rec_c, rb.sorted_splat, rb.ranges, order, out_rgb,        \
              rb.alphas, rb.last_ids, rb.width, rb.height, rb.ntx, rb.tile_inst, rb.geom,      \
-             L ? target : nullptr, L ? rb.loss_partials : nullptr, rb.scalars)
+             L ? target : nullptr, L ? rb.loss_partials : nullptr, rb.scalars, mode)
   if (count) DS_FWD(false, true);
   else if (target) DS_FWD(true, false);
   else DS_FWD(false, false);
@@ -679,7 +732,7 @@ void launch_fwd(RasterBuffers& rb, float* out_rgb, const float* target, bool cou
 
 template <int PPT, int TS, bool kBatch>
 void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, const float* target,
-                cudaStream_t s) {
+                cudaStream_t s, const DevScalars* mode = nullptr) {
   constexpr int NT = Lay<PPT, TS>::kThreads;
   const float* g = grad_rgb ? grad_rgb : image;
   const float* t = grad_rgb ? nullptr : target;
@@ -689,7 +742,7 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
   launch_pdl(composite_bwd_kernel<PPT, TS, F, E, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
              rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit,      \
              rb.ranges, order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width,         \
-             rb.height, rb.ntx, rb.tile_inst, rb.geom, rb.depth_keys, rb.tile_bound)
+             rb.height, rb.ntx, rb.tile_inst, rb.geom, rb.depth_keys, rb.tile_bound, mode)
   if (grad_rgb) {
     if (exact) DS_BWD(false, true);
     else DS_BWD(false, false);
@@ -728,7 +781,7 @@ struct BwdOp {
 // pixels with PPT 1 or 2.
 template <class F>
 int dispatch(const RasterBuffers& rb, const F& f, bool backward = false) {
-  const int ppt = backward ? rb.ppt_bwd : rb.ppt;
+  const int ppt = (backward && rb.ppt_bwd != 0) ? rb.ppt_bwd : rb.ppt;
   if (!rb.geom) {
     switch (ppt) {
       case 4: f.template run<4, 16, false>(); return DS_OK;
@@ -772,7 +825,8 @@ int composite_default_ppt_bwd() {
     int v = atoi(e);
     if (v == 1 || v == 2 || v == 4) return v;
   }
-  return composite_default_ppt();
+  // chosen per forward (kDenseLanesX10) behind a one-pixel-per-thread forward
+  return composite_default_ppt() == 1 ? 0 : composite_default_ppt();
 }
 
 bool composite_longest_first() {
@@ -797,7 +851,13 @@ int raster_composite_count(RasterBuffers& rb, float* out_rgb, cudaStream_t s) {
 
 int raster_composite_backward(RasterBuffers& rb, const float* image, const float* grad_rgb,
                               const float* target, cudaStream_t s) {
-  dispatch(rb, BwdOp{rb, image, grad_rgb, target, s}, true);
+  if (adaptive_bwd(rb)) {
+    // the launch of the layout the forward chose does the work
+    launch_bwd<2, 16, false>(rb, image, grad_rgb, target, s, rb.scalars);
+    launch_bwd<1, 16, false>(rb, image, grad_rgb, target, s, rb.scalars);
+  } else {
+    dispatch(rb, BwdOp{rb, image, grad_rgb, target, s}, true);
+  }
   return cuda_status(cudaGetLastError());
 }
 

@@ -149,6 +149,11 @@ struct DevScalars {
   float loss;
   float pad2;
   unsigned long long pairs[2];  // counting forward: contributing, tested (pixel, splat) pairs
+  // Backward layout of the last forward (ppt_bwd == 0): its hits and their
+  // contributing lanes summed over the CTAs, the last CTA's decision
+  unsigned long long mode_hits, mode_lanes;
+  uint32_t mode_ticket;
+  uint32_t bwd_ppt;  // 2: two pixels per thread; otherwise one
 };
 
 // ---------------------------------------------------------------------------
@@ -167,7 +172,10 @@ struct RasterBuffers {
   int64_t cap = 0;  // intersection capacity
   int grad_mode = DS_GRAD_REFERENCE;
   int ppt = 2;      // pixels per thread of the composite forward (1, 2 or 4)
-  int ppt_bwd = 2;  // pixels per thread of the composite backward
+  // pixels per thread of the composite backward (1, 2 or 4), or 0: chosen
+  // per forward, 2 when its hits covered the warps' pixel blocks densely and 1
+  // otherwise (single-instance 16-pixel tiles; DevScalars::bwd_ppt)
+  int ppt_bwd = 2;
   int schedule = DS_SCHEDULE_LONGEST_FIRST;  // composite tile order
   int tile_size = 16;  // pixels per tile edge: 16 (reference); batches may use 8 or 32
 

@@ -151,7 +151,7 @@ extern "C" int ds_raster_forward_noalloc(const ds_splat2d* in, int width, int he
   rb.max_splats = kMaxSplats;
   rb.cap = kMaxIsects;
   rb.ppt = composite_default_ppt();
-  rb.ppt_bwd = composite_default_ppt_bwd();
+  rb.ppt_bwd = rb.ppt;  // forward only: no backward layout to choose
   const size_t n = kMaxSplats;
   rb.rec_a = c.take<float4>(16 * n);
   rb.rec_b = c.take<float4>(16 * n);
