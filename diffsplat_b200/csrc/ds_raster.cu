@@ -436,8 +436,15 @@ __global__ void __launch_bounds__(kOffsetThreads)
   if (threadIdx.x == 0) sc->sort_ticket = 0u;
 }
 
-// blockDim.x = 32 * warps; dynamic shared memory (1 + warps) * tiles * 4 B.
-__global__ void __launch_bounds__(kThreads)
+// kScatterWarps warps per CTA; dynamic shared memory tiles * (4 + 2 *
+// kScatterWarps) B: the tiles' bases and each warp's 16-bit offsets inside
+// the chunk.  A chunk of more than 65535 pairs (only when the live pair count
+// exceeds kSortBlocks * 65535) does not fit 16-bit offsets: warp 0 then walks
+// the whole chunk alone with 32-bit counters in the same shared memory.
+constexpr int kScatterWarps = 8;
+constexpr uint32_t kScatterChunk16 = 65535;
+
+__global__ void __launch_bounds__(32 * kScatterWarps)
     tile_scatter_kernel(const uint32_t* __restrict__ tile_keys,
                         const uint32_t* __restrict__ emit_splat, const uint32_t* __restrict__ n_dev,
                         int tiles, const uint32_t* __restrict__ hist,
@@ -445,51 +452,62 @@ __global__ void __launch_bounds__(kThreads)
                         uint32_t* __restrict__ sorted_emit) {
   pdl_wait();
   extern __shared__ uint32_t smem[];
-  const int warps = blockDim.x >> 5;
-  uint32_t* base = smem;          // [tiles]: range start + chunk prefix
-  uint32_t* woff = smem + tiles;  // [warps][tiles]: warp counts, then warp prefixes
+  constexpr int NT = 32 * kScatterWarps;
+  uint32_t* base = smem;                                         // [tiles]
+  uint16_t* woff = reinterpret_cast<uint16_t*>(smem + tiles);   // [warps][tiles]
+  uint32_t* wide = smem + tiles;                                 // [tiles] (large chunks)
   uint32_t lo, hi;
   chunk_of(*n_dev, gridDim.x, blockIdx.x, lo, hi);
   if (lo >= hi) return;  // uniform
+  const bool big = hi - lo > kScatterChunk16;  // uniform
+  const int warps = big ? 1 : kScatterWarps;
   const uint32_t* prefix = hist + (size_t)blockIdx.x * tiles;
-  for (int t = threadIdx.x; t < tiles; t += blockDim.x) base[t] = (uint32_t)ranges[t].x + prefix[t];
-  for (int q = threadIdx.x; q < warps * tiles; q += blockDim.x) woff[q] = 0u;
+  for (int t = threadIdx.x; t < tiles; t += NT) base[t] = (uint32_t)ranges[t].x + prefix[t];
+  if (big) {
+    for (int t = threadIdx.x; t < tiles; t += NT) wide[t] = 0u;
+  } else {
+    for (int q = threadIdx.x; q < (kScatterWarps * tiles + 1) / 2; q += NT) wide[q] = 0u;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const uint32_t per = (hi - lo + warps - 1) / warps;
-  const uint32_t wlo = min(hi, lo + w * per), whi = min(hi, wlo + per);
-  uint32_t* mine = woff + (size_t)w * tiles;
   const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t per = (hi - lo + warps - 1) / warps;
+  const uint32_t wlo = w < warps ? min(hi, lo + w * per) : hi, whi = min(hi, wlo + per);
+  uint16_t* mine = woff + (size_t)w * tiles;
   // The run is walked kAhead warp-steps at a time with all their loads issued
   // first: the steps depend on one another only through the shared counters.
   constexpr int kAhead = 8;
-  // 1) pairs per tile in this warp's run
-  for (uint32_t e0 = wlo; e0 < whi; e0 += 32 * kAhead) {
-    uint32_t tk[kAhead];
+  if (!big) {
+    // 1) pairs per tile in this warp's run
+    for (uint32_t e0 = wlo; e0 < whi; e0 += 32 * kAhead) {
+      uint32_t tk[kAhead];
 #pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const uint32_t e = e0 + 32 * u + lane;
-      tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
-    }
+      for (int u = 0; u < kAhead; ++u) {
+        const uint32_t e = e0 + 32 * u + lane;
+        tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
+      }
 #pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const uint32_t t = tk[u];
-      const uint32_t peers = __match_any_sync(0xffffffffu, t);
-      if (t < (uint32_t)tiles && (peers & lt) == 0u) mine[t] += (uint32_t)__popc(peers);
-      __syncwarp();
+      for (int u = 0; u < kAhead; ++u) {
+        const uint32_t t = tk[u];
+        const uint32_t peers = __match_any_sync(0xffffffffu, t);
+        if (t < (uint32_t)tiles && (peers & lt) == 0u)
+          mine[t] = (uint16_t)(mine[t] + __popc(peers));
+        __syncwarp();
+      }
     }
-  }
-  __syncthreads();
-  // 2) exclusive prefix over the warps, per tile
-  for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
-    uint32_t run = 0;
-    for (int k = 0; k < warps; ++k) {
-      const uint32_t c = woff[(size_t)k * tiles + t];
-      woff[(size_t)k * tiles + t] = run;
-      run += c;
+    __syncthreads();
+    // 2) exclusive prefix over the warps, per tile (at most the chunk size)
+    for (int t = threadIdx.x; t < tiles; t += NT) {
+      uint32_t run = 0;
+#pragma unroll
+      for (int k = 0; k < kScatterWarps; ++k) {
+        const uint32_t c = woff[(size_t)k * tiles + t];
+        woff[(size_t)k * tiles + t] = (uint16_t)run;
+        run += c;
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
   // 3) each pair to its slot, in order
   for (uint32_t e0 = wlo; e0 < whi; e0 += 32 * kAhead) {
     uint32_t tk[kAhead], sp[kAhead];
@@ -507,8 +525,14 @@ __global__ void __launch_bounds__(kThreads)
       const bool valid = t < (uint32_t)tiles;  // false past the run's end
       uint32_t p0 = 0;
       if (valid && lane == leader) {
-        p0 = base[t] + mine[t];
-        mine[t] += (uint32_t)__popc(peers);
+        const uint32_t n_peers = (uint32_t)__popc(peers);
+        if (big) {
+          p0 = base[t] + wide[t];
+          wide[t] += n_peers;
+        } else {
+          p0 = base[t] + mine[t];
+          mine[t] = (uint16_t)(mine[t] + n_peers);
+        }
       }
       p0 = __shfl_sync(0xffffffffu, p0, leader);
       if (valid) {
@@ -520,9 +544,6 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
 }
-
-// Warps per scatter CTA: as many as keep three CTAs per SM within 227 KB.
-inline int scatter_warps(int tiles) { return tiles <= 2048 ? 8 : (tiles <= 4096 ? 4 : 2); }
 
 // Longest-first schedule of the composite CTAs: tiles bucketed by their list
 // length (quarter-octave buckets), buckets in descending order.  The heaviest
@@ -671,7 +692,7 @@ static int alloc_count_sort(RasterBuffers& rb) {
   int dev = 0;
   DS_CUDA(cudaGetDevice(&dev));
   if (dev >= 64 || !(smem_set >> dev & 1u)) {
-    const int most = kCountSortMaxTiles * 4 * (1 + scatter_warps(kCountSortMaxTiles));
+    const int most = kCountSortMaxTiles * (4 + 2 * kScatterWarps);
     DS_CUDA(cudaFuncSetAttribute(tile_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  most));
     if (dev < 64) smem_set |= 1ull << dev;
@@ -802,14 +823,15 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
     if (rb.tile_hist) {
       // 4) stable counting sort by tile id; the ranges come out of its scan
-      const int T = rb.tiles, G = rb.count_chunks, W = scatter_warps(T);
+      const int T = rb.tiles, G = rb.count_chunks;
       const size_t cnt_smem = (size_t)T * 4;
-      const size_t sct_smem = (size_t)T * 4 * (1 + W);
+      const size_t sct_smem = (size_t)T * (4 + 2 * kScatterWarps);
       DS_CUDA(launch_pdl(tile_count_kernel, dim3(G), dim3(kThreads), cnt_smem, s, rb.tile_k0,
                          &sc->n_isects, T, rb.tile_hist, &sc->status));
       DS_CUDA(launch_pdl(tile_offsets_kernel, dim3((T + 31) / 32), dim3(kOffsetThreads), 0, s,
                          rb.tile_hist, G, T, rb.tile_totals, rb.ranges, sc));
-      DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * W), sct_smem, s, rb.tile_k0,
+      DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * kScatterWarps), sct_smem, s,
+                         rb.tile_k0,
                          rb.emit_splat, &sc->n_isects, T, rb.tile_hist, rb.ranges,
                          rb.sorted_splat, rb.tile_v0));
       rb.sorted_emit = rb.tile_v0;
