@@ -103,6 +103,7 @@ _SIGS = {
     "ds_abi_version": (C.c_int, []),
     "ds_status_string": (C.c_char_p, [C.c_int]),
     "ds_device_check": (C.c_int, []),
+    "ds_debug_fail_allocations_after": (C.c_int, [C.c_int64]),
     "ds_activ_forward": (C.c_int, [C.POINTER(Gaussian3D), C.c_int, _fp, C.POINTER(Splat3D), _vp]),
     "ds_activ_backward": (C.c_int, [C.POINTER(Gaussian3D), C.POINTER(Splat3D), C.POINTER(Splat3D),
                                     C.c_int, _fp, C.POINTER(Gaussian3D), _vp]),
@@ -166,6 +167,7 @@ _SIGS = {
     "ds_gemm_bf16_tn": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int, _vp,
                                   _vp, _vp]),
+    "ds_gemm_set_spin_limit": (C.c_int, [C.c_uint32]),
     "ds_im2col_bf16": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
                                  _vp]),
     "ds_col2im_bf16": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp,

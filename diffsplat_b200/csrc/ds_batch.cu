@@ -235,15 +235,15 @@ int ds_batch_create(const ds_batch_config* cfg, const ds_batch_instance* inst, d
   const bool bf16 = cfg->storage == DS_STORAGE_BF16;
   const size_t mom = b->floats * (bf16 ? 2 : 4);
   int st;
-  if ((st = ds::cuda_status(cudaMalloc(&b->params_mem, b->floats * 4)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->m_mem, mom)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->v_mem, mom)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->params_mem, b->floats * 4)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->m_mem, mom)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->v_mem, mom)))) return fail(st);
   cudaMemset(b->params_mem, 0, b->floats * 4);
   cudaMemset(b->m_mem, 0, mom);
   cudaMemset(b->v_mem, 0, mom);
   ds::carve(b->params_mem, n, b->bands, b->P);
   if (bf16) {
-    if ((st = ds::cuda_status(cudaMalloc(&b->render_mem, b->floats * 2)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&b->render_mem, b->floats * 2)))) return fail(st);
     cudaMemset(b->render_mem, 0, b->floats * 2);
     ds::carve_soa(b->render_mem, n, b->bands, b->R16);
     ds::carve_soa((__nv_bfloat16*)b->m_mem, n, b->bands, b->M16);
@@ -252,9 +252,9 @@ int ds_batch_create(const ds_batch_config* cfg, const ds_batch_instance* inst, d
     ds::carve((float*)b->m_mem, n, b->bands, b->M);
     ds::carve((float*)b->v_mem, n, b->bands, b->V);
   }
-  if ((st = ds::cuda_status(cudaMalloc(&b->targets, (size_t)pixels * 12)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->images, (size_t)pixels * 12)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->losses, (size_t)I * 4)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->targets, (size_t)pixels * 12)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->images, (size_t)pixels * 12)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->losses, (size_t)I * 4)))) return fail(st);
   cudaMemset(b->targets, 0, (size_t)pixels * 12);
   cudaMemset(b->images, 0, (size_t)pixels * 12);
   cudaMemset(b->losses, 0, (size_t)I * 4);
@@ -266,11 +266,11 @@ int ds_batch_create(const ds_batch_config* cfg, const ds_batch_instance* inst, d
     std::fill(tinst.begin() + g.tile_off, tinst.begin() + g.tile_off + g.ntx * g.nty,
               (uint16_t)k);
   }
-  if ((st = ds::cuda_status(cudaMalloc(&b->inst_of_splat, sinst.size() * 2)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->tile_inst, tinst.size() * 2)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->geom_dev, (size_t)I * sizeof(ds::InstGeom)))))
+  if ((st = ds::cuda_status(ds::device_alloc(&b->inst_of_splat, sinst.size() * 2)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->tile_inst, tinst.size() * 2)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->geom_dev, (size_t)I * sizeof(ds::InstGeom)))))
     return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->cams, (size_t)I * sizeof(ds::Camera))))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->cams, (size_t)I * sizeof(ds::Camera))))) return fail(st);
   cudaMemcpy(b->inst_of_splat, sinst.data(), sinst.size() * 2, cudaMemcpyHostToDevice);
   cudaMemcpy(b->tile_inst, tinst.data(), tinst.size() * 2, cudaMemcpyHostToDevice);
   cudaMemcpy(b->geom_dev, b->geom.data(), (size_t)I * sizeof(ds::InstGeom),
@@ -287,7 +287,7 @@ int ds_batch_create(const ds_batch_config* cfg, const ds_batch_instance* inst, d
   b->rb.geom = b->geom_dev;
   b->rb.instances = I;
   if ((st = ds::make_bc_table(cfg->beta1, cfg->beta2, &b->bc_table, &b->bc_len))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&b->bc_cur, sizeof(float2))))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&b->bc_cur, sizeof(float2))))) return fail(st);
   uint32_t nn = (uint32_t)n;
   cudaMemcpy(&b->rb.scalars->n_splats, &nn, sizeof(uint32_t), cudaMemcpyHostToDevice);
   if ((st = ds::cuda_status(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking))))

@@ -2,6 +2,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <atomic>
 #include <new>
 #include <vector>
 
@@ -47,9 +48,30 @@ bool s2_ok(const ds_splat2d* s) {
 
 namespace {
 int g_default_grad_mode = -1;  // -1: not yet read from the environment
+// Successful device allocations left before they fail; -1: no limit.
+std::atomic<int64_t> g_alloc_budget{-1};
 }
 
+namespace ds {
+cudaError_t device_alloc_bytes(void** p, size_t bytes) {
+  int64_t left = g_alloc_budget.load();
+  while (left >= 0) {
+    if (left == 0) {
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+    if (g_alloc_budget.compare_exchange_weak(left, left - 1)) break;
+  }
+  return cudaMalloc(p, bytes);
+}
+}  // namespace ds
+
 extern "C" {
+
+int ds_debug_fail_allocations_after(int64_t n) {
+  g_alloc_budget.store(n < 0 ? -1 : n);
+  return DS_OK;
+}
 
 int ds_default_grad_mode(void) {
   if (g_default_grad_mode < 0) {

@@ -196,15 +196,15 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
   };
   const bool bf16 = cfg->storage == DS_STORAGE_BF16;
   const size_t mom_bytes = f->floats * (bf16 ? 2 : 4);
-  if ((st = ds::cuda_status(cudaMalloc(&f->params_mem, f->floats * 4)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->m_mem, mom_bytes)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->v_mem, mom_bytes)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->params_mem, f->floats * 4)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->m_mem, mom_bytes)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->v_mem, mom_bytes)))) return fail(st);
   cudaMemset(f->params_mem, 0, f->floats * 4);
   cudaMemset(f->m_mem, 0, mom_bytes);
   cudaMemset(f->v_mem, 0, mom_bytes);
   ds::carve(f->params_mem, n, f->bands, f->P);
   if (bf16) {
-    if ((st = ds::cuda_status(cudaMalloc(&f->render_mem, f->floats * 2)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&f->render_mem, f->floats * 2)))) return fail(st);
     cudaMemset(f->render_mem, 0, f->floats * 2);
     ds::carve_soa(f->render_mem, n, f->bands, f->R16);
     ds::carve_soa((__nv_bfloat16*)f->m_mem, n, f->bands, f->M16);
@@ -215,31 +215,31 @@ static int ds_fitter_create_impl(const ds_fitter_config* cfg, int keep_grads, ds
     ds::carve(f->v_mem, n, f->bands, f->V);
   }
   if (keep_grads) {
-    if ((st = ds::cuda_status(cudaMalloc(&f->g_mem, f->floats * 4)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&f->g_mem, f->floats * 4)))) return fail(st);
     cudaMemset(f->g_mem, 0, f->floats * 4);
     ds::carve(f->g_mem, n, f->bands, f->G);
   } else {
     f->G = f->P;  // never written (keep_grads == 0)
   }
   const size_t px = (size_t)cfg->width * cfg->height;
-  if ((st = ds::cuda_status(cudaMalloc(&f->target, px * 3 * 4)))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->image, px * 3 * 4)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->target, px * 3 * 4)))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->image, px * 3 * 4)))) return fail(st);
   cudaMemset(f->image, 0, px * 3 * 4);
   f->capacity = std::max(n, cfg->capacity);
   if ((st = ds::raster_alloc(f->rb, cfg->width, cfg->height, f->capacity, cfg->max_isects)))
     return fail(st);
   if (f->capacity > n) {
-    if ((st = ds::cuda_status(cudaMalloc(&f->grad_accum, (size_t)f->capacity * 4)))) return fail(st);
-    if ((st = ds::cuda_status(cudaMalloc(&f->grad_count, (size_t)f->capacity * 4)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&f->grad_accum, (size_t)f->capacity * 4)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&f->grad_count, (size_t)f->capacity * 4)))) return fail(st);
     cudaMemset(f->grad_accum, 0, (size_t)f->capacity * 4);
     cudaMemset(f->grad_count, 0, (size_t)f->capacity * 4);
   }
   f->rb.grad_mode = cfg->grad_mode;
   f->rb.schedule = cfg->schedule;
-  if ((st = ds::cuda_status(cudaMalloc(&f->cam_dev, sizeof(ds::Camera))))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->cam_dev, sizeof(ds::Camera))))) return fail(st);
   cudaMemset(f->cam_dev, 0, sizeof(ds::Camera));
   if ((st = ds::make_bc_table(cfg->beta1, cfg->beta2, &f->bc_table, &f->bc_len))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&f->bc_cur, sizeof(float2))))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&f->bc_cur, sizeof(float2))))) return fail(st);
   // The depth sort reads its element count from device memory.
   uint32_t nn = (uint32_t)n;
   cudaMemcpy(&f->rb.scalars->n_splats, &nn, sizeof(uint32_t), cudaMemcpyHostToDevice);
@@ -546,13 +546,13 @@ int ds_fitter_densify(ds_fitter* f, const ds_densify_params* p, int32_t* new_cou
     cleanup();
     return code;
   };
-  if ((st = ds::cuda_status(cudaMalloc(&mode, n))) ||
-      (st = ds::cuda_status(cudaMalloc(&emit, (size_t)n * 4))) ||
-      (st = ds::cuda_status(cudaMalloc(&iota, (size_t)n * 4))) ||
-      (st = ds::cuda_status(cudaMalloc(&offs, (size_t)n * 8))) ||
-      (st = ds::cuda_status(cudaMalloc(&total, 8))) ||
-      (st = ds::cuda_status(cudaMalloc(&total32, 4))) ||
-      (st = ds::cuda_status(cudaMalloc(&status, 4))))
+  if ((st = ds::cuda_status(ds::device_alloc(&mode, n))) ||
+      (st = ds::cuda_status(ds::device_alloc(&emit, (size_t)n * 4))) ||
+      (st = ds::cuda_status(ds::device_alloc(&iota, (size_t)n * 4))) ||
+      (st = ds::cuda_status(ds::device_alloc(&offs, (size_t)n * 8))) ||
+      (st = ds::cuda_status(ds::device_alloc(&total, 8))) ||
+      (st = ds::cuda_status(ds::device_alloc(&total32, 4))) ||
+      (st = ds::cuda_status(ds::device_alloc(&status, 4))))
     return fail(st);
   std::vector<uint32_t> h_iota(n);
   for (int k = 0; k < n; ++k) h_iota[k] = (uint32_t)k;
@@ -572,9 +572,9 @@ int ds_fitter_densify(ds_fitter* f, const ds_densify_params* p, int32_t* new_cou
   if (h_total == 0 || h_total > (unsigned long long)f->capacity) return fail(DS_ERR_OOM);
   const int n2 = (int)h_total;
   const size_t floats = (size_t)n2 * (14 + 3 * f->bands);
-  if ((st = ds::cuda_status(cudaMalloc(&np, floats * 4))) ||
-      (st = ds::cuda_status(cudaMalloc(&nm, floats * 4))) ||
-      (st = ds::cuda_status(cudaMalloc(&nv, floats * 4))))
+  if ((st = ds::cuda_status(ds::device_alloc(&np, floats * 4))) ||
+      (st = ds::cuda_status(ds::device_alloc(&nm, floats * 4))) ||
+      (st = ds::cuda_status(ds::device_alloc(&nv, floats * 4))))
     return fail(st);
   ds_gaussian3d Q, MQ, VQ;
   ds::carve(np, n2, f->bands, Q);

@@ -13,7 +13,11 @@
 //   warps 0-3      epilogue: tcgen05.ld 32 lanes x 32 columns per warp and
 //                  step, fused bias / GELU, stores to global memory
 // Every mbarrier wait is bounded; on timeout the CTA records an error code,
-// drains what it issued (bounded again), frees its TMEM and returns.
+// drains what it issued (bounded again), frees its TMEM and returns.  The
+// pipeline waits poll up to a runtime limit (ds_gemm_set_spin_limit); the
+// drain always polls up to kSpinLimit, so the copies and MMAs a CTA issued
+// have landed before it frees its TMEM and shared memory even when the
+// pipeline limit was set low.
 // Split-K (blockIdx.z) writes FP32 partials that gemm_reduce_splits sums in
 // a fixed order.
 #include <cuda.h>
@@ -30,7 +34,8 @@ namespace ds {
 namespace {
 
 constexpr int kBM = 128, kBK = 64, kStages = 4, kGemmThreads = 128;
-constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr uint32_t kSpinLimit = 1u << 24;  // default pipeline limit and the drain's limit
+uint32_t g_spin_limit = kSpinLimit;
 
 enum Epilogue : int { kEpiF32 = 0, kEpiBiasGeluBf16 = 1, kEpiBiasF32 = 2 };
 
@@ -44,6 +49,7 @@ struct GemmArgs {
   int ldy;
   const float* bias;  // [N] or null
   uint32_t* err;      // set non-zero when a wait times out
+  uint32_t spin;      // polls per pipeline wait
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -61,9 +67,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kSpinLimit) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     for (int i = 0; i < nkb; ++i) {
       const int s = i % kStages;
       const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-      if (!mbar_wait(&empty[s], ph ^ 1u)) {
+      if (!mbar_wait(&empty[s], ph ^ 1u, g.spin)) {
         atomicExch(&failed, 1);
         break;
       }
@@ -214,7 +221,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     for (int i = 0; i < nkb; ++i) {
       const int s = i % kStages;
       const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-      if (!mbar_wait(&full[s], ph)) {
+      if (!mbar_wait(&full[s], ph, g.spin)) {
         atomicExch(&failed, 1);
         break;
       }
@@ -231,7 +238,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   __syncwarp();
 
   // epilogue: every warp reads its 32 TMEM lanes (= rows m0 + 32 warp + lane)
-  const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0, g.spin));
   if (!ok) atomicExch(&failed, 1);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const int row = m0 + warp * 32 + lane;
@@ -281,9 +288,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (failed) {
-    // drain the copies this CTA issued before freeing its shared memory
+    // Drain before freeing TMEM and shared memory: the copies still in flight
+    // (at most the last kStages issued: an earlier stage was reused only
+    // after its copy had landed and been consumed) and the MMAs the issuer
+    // committed to `done`.
     if (warp == 0 && lane == 0) {
-      for (int i = 0; i < issued; ++i) mbar_wait(&full[i % kStages], (uint32_t)(i / kStages) & 1u);
+      for (int i = max(0, issued - kStages); i < issued; ++i)
+        mbar_wait(&full[i % kStages], (uint32_t)(i / kStages) & 1u, kSpinLimit);
+      mbar_wait(done, 0, kSpinLimit);
       atomicOr(g.err, 1u);
     }
     __syncthreads();
@@ -598,6 +610,7 @@ int ds_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb, int M, int N
   g.ldy = ldy;
   g.bias = bias;
   g.err = err;
+  g.spin = ds::g_spin_limit;
   cudaStream_t s = (cudaStream_t)stream;
   int st;
   switch (epilogue) {
@@ -611,6 +624,11 @@ int ds_gemm_bf16_tn(const void* A, int lda, const void* B, int ldb, int M, int N
                                                                         splits);
     DS_CUDA(cudaGetLastError());
   }
+  return DS_OK;
+}
+
+int ds_gemm_set_spin_limit(uint32_t polls) {
+  ds::g_spin_limit = polls == 0 ? ds::kSpinLimit : polls;
   return DS_OK;
 }
 

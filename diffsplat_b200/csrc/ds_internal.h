@@ -23,6 +23,15 @@ inline int cuda_status(cudaError_t e) {
 
 #define DS_CUDA(expr) DS_TRY(::ds::cuda_status(expr))
 
+// Every device allocation of the library goes through device_alloc, so that a
+// test can make the allocations after a given count fail as out of memory
+// (ds_debug_fail_allocations_after) and exercise each clean-up path.
+cudaError_t device_alloc_bytes(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t device_alloc(T** p, size_t bytes) {
+  return device_alloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+
 // Launches `kernel` with programmatic dependent launch: its CTAs may be
 // scheduled while the previous kernel in the stream finishes, and it waits
 // for that kernel (pdl_wait) before its first memory access.

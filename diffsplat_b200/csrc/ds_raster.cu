@@ -613,7 +613,7 @@ template <typename T>
 int alloc(T** p, size_t n) {
   *p = nullptr;
   if (n == 0) n = 1;
-  return cuda_status(cudaMalloc((void**)p, n * sizeof(T)));
+  return cuda_status(ds::device_alloc((void**)p, n * sizeof(T)));
 }
 
 template <typename T>

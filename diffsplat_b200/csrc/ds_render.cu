@@ -56,14 +56,14 @@ int ds_renderer_create(int width, int height, int max_splats, int sh_degree, int
   r->bands = ds::sh_bands(sh_degree);
   int st;
   if ((st = ds::raster_alloc(r->rb, width, height, max_splats, max_isects))) return fail(st);
-  if ((st = ds::cuda_status(cudaMalloc(&r->cam_dev, sizeof(ds::Camera))))) return fail(st);
+  if ((st = ds::cuda_status(ds::device_alloc(&r->cam_dev, sizeof(ds::Camera))))) return fail(st);
   cudaMemset(r->cam_dev, 0, sizeof(ds::Camera));
-  if ((st = ds::cuda_status(cudaMalloc(&r->image, image_floats(width, height) * 4))))
+  if ((st = ds::cuda_status(ds::device_alloc(&r->image, image_floats(width, height) * 4))))
     return fail(st);
   cudaMemset(r->image, 0, image_floats(width, height) * 4);
   if (storage == DS_STORAGE_BF16) {
     r->copy_elems = (size_t)max_splats * (14 + 3 * r->bands);
-    if ((st = ds::cuda_status(cudaMalloc(&r->copy_mem, r->copy_elems * 2)))) return fail(st);
+    if ((st = ds::cuda_status(ds::device_alloc(&r->copy_mem, r->copy_elems * 2)))) return fail(st);
   }
   if ((st = ds::cuda_status(cudaDeviceSynchronize()))) return fail(st);
   *out = r;
@@ -155,7 +155,7 @@ int ds_renderer_resize(ds_renderer* r, int width, int height) {
   DS_TRY(ds::raster_resize(r->rb, width, height));
   cudaFree(r->image);
   r->image = nullptr;
-  DS_CUDA(cudaMalloc(&r->image, image_floats(width, height) * 4));
+  DS_CUDA(ds::device_alloc(&r->image, image_floats(width, height) * 4));
   DS_CUDA(cudaMemset(r->image, 0, image_floats(width, height) * 4));
   return DS_OK;
 }

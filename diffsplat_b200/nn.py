@@ -58,6 +58,15 @@ class Gemm:
         if int(self.err.item()) != 0:
             raise RuntimeError("tensor-core GEMM pipeline wait timed out")
 
+    def clear(self):
+        self.err.zero_()
+
+
+def set_spin_limit(polls: int = 0) -> None:
+    """Polls per pipeline wait of the GEMM before it reports a timeout
+    (0: the default).  Lowered only to test the timeout path."""
+    L.call("ds_gemm_set_spin_limit", polls)
+
 
 def kpad(c_in: int) -> int:
     """im2col width: 9 * c_in rounded up to 64 (one 128-byte K block)."""

@@ -97,6 +97,12 @@ typedef struct ds_splat2d {
 int ds_set_default_grad_mode(int mode);
 int ds_default_grad_mode(void);
 
+/* Test hook for failure detection (no reference counterpart): after n more
+ * successful device allocations, the library's next ones fail as if the
+ * device were out of memory, so every create / densify call can be driven
+ * through its clean-up path; n < 0 turns this off.  Process-wide. */
+int ds_debug_fail_allocations_after(int64_t n);
+
 /* Library information. */
 int ds_abi_version(void);
 const char *ds_status_string(int status);
@@ -373,6 +379,12 @@ int ds_batch_destroy(ds_batch *b);
 int ds_gemm_bf16_tn(const void *A, int lda, const void *B, int ldb, int M, int N, int K,
                     int epilogue, float *D, int ldd, void *Y, void *Z, int ldy, const float *bias,
                     int splits, float *workspace, uint32_t *err, ds_stream stream);
+/* Polls each pipeline wait of ds_gemm_bf16_tn makes before it gives up and
+ * reports through *err (process-wide; 0 restores the default of 2^24, which
+ * no healthy pipeline reaches).  A low limit exercises that failure path: the
+ * CTAs still let what they issued land before they free their TMEM and
+ * shared memory, and the device stays usable.  No reference counterpart. */
+int ds_gemm_set_spin_limit(uint32_t polls);
 /* 3x3 convolution with padding 1 and stride 1 or 2 on NHWC BF16 tensors:
  * im2col writes col[B*Ho*Wo][Kp] (k = (ky*3 + kx)*C + c, zero for k >= 9C);
  * col2im sums dcol back onto dx[B][H][W][C] and multiplies by gelu'(z) when z

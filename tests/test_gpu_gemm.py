@@ -80,3 +80,30 @@ def test_conv_forward_backward_matches_fp32(cuda_lib, cin, cout, stride, H):
     gref = torch.autograd.grad(F.gelu(zp, approximate="tanh"), zp, xr.grad)[0]
     assert _rel(dx.permute(0, 3, 1, 2), gref) < 1e-2
     assert (conv.gw[:, 9 * cin:] == 0).all()
+
+
+def test_pipeline_wait_timeout_is_reported_and_device_stays_usable(cuda_lib):
+    """Failure detection without a GPU fault: with the pipeline waits limited
+    to one poll, the TMA copies cannot land in time, so the CTAs give up,
+    let what they issued land, free their TMEM and set the error word that
+    Gemm.check() turns into an exception.  The next GEMM with the default
+    limit on the same context is correct."""
+    import torch
+    from diffsplat_b200 import nn
+    g = torch.Generator().manual_seed(11)
+    A = torch.randn(2048, 1152, generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn(256, 1152, generator=g).to(torch.bfloat16).cuda()
+    gemm = nn.Gemm()
+    nn.set_spin_limit(1)
+    try:
+        gemm(A, B)
+        torch.cuda.synchronize()
+    finally:
+        nn.set_spin_limit(0)
+    with pytest.raises(RuntimeError, match="timed out"):
+        gemm.check()
+    gemm.clear()
+    D = gemm(A, B)
+    torch.cuda.synchronize()
+    gemm.check()
+    assert _rel(D, A.float() @ B.float().T) < 2e-3
