@@ -514,6 +514,20 @@ def run_init(args) -> dict:
     t_train = time.perf_counter() - t0
     held = targets[n_train:]
     ev = I.evaluate(init, held, goal=28.0, max_steps=2000)
+    # final PSNR at an equal step budget, the three inits side by side
+    equal = {"steps": 2000, "random": [], "grid": [], "learned": []}
+    grid0 = init.zero_params(1)
+    for k in range(len(held)):
+        t = held[k]
+        for arm, p0 in (("random", I.random_init(init, k)), ("grid", grid0),
+                        ("learned", init.predict(t))):
+            r = I.steps_to_psnr(p0, t, init, goal=1e9, max_steps=equal["steps"], check_every=500)
+            equal[arm].append(r["psnr"])
+    for arm in ("random", "grid", "learned"):
+        equal[f"{arm}_mean"] = float(np.mean(equal[arm]))
+    d = np.array(equal["learned"]) - np.array(equal["random"])
+    equal["learned_minus_random_mean"] = float(d.mean())
+    equal["learned_minus_random_min"] = float(d.min())
     # learned init + batched BF16 fitting of all held-out targets together
     a.record()
     out = init.forward(held.contiguous())
@@ -548,6 +562,7 @@ def run_init(args) -> dict:
             "bf16_peak_tflops": peaks.get("bf16_tflops"),
             "gemm_frac_8192cubed": big / peaks.get("bf16_tflops", 1590.0),
             "eval": {k: v for k, v in ev.items() if k != "rows"},
+            "equal_steps_final_psnr": equal,
             "learned_batched_bf16_seconds_all": batch_s, "learned_batched_steps": steps,
             "learned_batched_psnr_min": min(final),
             "random_fp32_sequential_seconds_all": ev["random_seconds"] * n_eval,

@@ -291,7 +291,8 @@ def evaluate(init: Initializer, targets, goal: float = 28.0, max_steps: int = 20
         rnd = steps_to_psnr(random_init(init, seed * 7919 + k), t, init, goal, max_steps)
         grd = steps_to_psnr(grid, t, init, goal, max_steps)
         lrn = steps_to_psnr(P_learn, t, init, goal, max_steps)
-        fallback = lrn["psnr_first"] < rnd["psnr_first"]
+        # a NaN first PSNR (a prediction that does not render) falls back too
+        fallback = not (lrn["psnr_first"] >= rnd["psnr_first"])
         if fallback:
             lrn = dict(rnd)
         lrn["seconds"] += net_s

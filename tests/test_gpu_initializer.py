@@ -2,7 +2,8 @@
 bias gradient against the FP64 CPU oracle of the same network
 (oracle/initializer_oracle.py, BF16 weights, FP64 arithmetic; tolerances 3e-2
 relative for the BF16-activation forward, 5e-2 for gradients), the head
-decode, and that training lowers both loss terms."""
+decode, that training lowers both loss terms, what the trained network gains
+over the fitter without it, and the fallback to random init."""
 import numpy as np
 import pytest
 
@@ -70,3 +71,51 @@ def test_training_lowers_both_losses(cuda_lib):
     hist = I.train(init, targets, fitted, steps=60, batch=8, lr=1e-3, log_every=59)
     (_, l1a, ra), (_, l1b, rb) = hist[0], hist[-1]
     assert l1b < l1a and rb < ra, hist
+
+
+@pytest.fixture(scope="module")
+def trained_128(cuda_lib):
+    """A 128 x 128 initializer (16 x 16 grid, 1024 splats) trained on 96
+    targets whose splats the batched fitter fitted for 300 steps; 4 further
+    targets held out."""
+    from diffsplat_b200 import initializer as I
+    init = I.Initializer(size=128, seed=0)
+    targets = I.make_targets(100, size=128, seed=21)
+    fitted = I.fit_pairs(init, targets[:96], steps=300, batch=32)
+    I.train(init, targets[:96], fitted, steps=300, batch=16, lr=1e-3)
+    return init, targets[96:]
+
+
+def test_learned_init_reaches_the_goal_sooner_than_random_and_grid(trained_128):
+    """What the trained network gains over the method without it: on held-out
+    targets the learned init reaches 24 dB in fewer fitter steps and fewer
+    device seconds (network forward included) than the plain fitter's random
+    init and than the grid init (the zero-head output: the same fitter and
+    splat layout without the network), and needs no fallback."""
+    from diffsplat_b200 import initializer as I
+    init, held = trained_128
+    ev = I.evaluate(init, held, goal=24.0, max_steps=600)
+    assert ev["fallbacks"] == 0
+    assert ev["learned_reached"] == len(held)
+    assert ev["learned_steps"] < ev["grid_steps"] < ev["random_steps"], ev
+    assert ev["learned_seconds"] < ev["grid_seconds"], ev
+    assert ev["learned_seconds"] < ev["random_seconds"], ev
+
+
+def test_fallback_to_random_when_the_prediction_is_worse(cuda_lib):
+    """A prediction that renders worse than random init is not used:
+    evaluate() falls back to the random init, which then is the learned row.
+    The prediction here puts every splat behind the camera, so its image
+    stays black, on bright targets (black is 0.7 and 1.4 dB from them)."""
+    import numpy as np
+    from diffsplat_b200 import initializer as I
+    init = I.Initializer(size=64, seed=4)
+    bad = init.zero_params(1)
+    bad[2] = -4.0  # z < 0: every splat culled
+    init.predict = lambda image: bad
+    targets = np.stack([I.make_targets(2, size=64, seed=5)[0],
+                        I.make_targets(2, size=64, seed=6)[0]])
+    ev = I.evaluate(init, targets, goal=22.0, max_steps=100)
+    assert ev["fallbacks"] == 2, ev
+    assert ev["learned_steps"] == ev["random_steps"]
+    assert ev["learned_psnr_first"] == ev["random_psnr_first"]
