@@ -68,7 +68,11 @@ struct Lay {
   static constexpr int kBwdBatch = 1024 / kWarps < 128 ? 1024 / kWarps : 128;
   // resident CTAs per SM the register allocation must allow (256-thread CTAs)
   static constexpr int kMinBlocksFwd = kThreads == 256 ? DS_FWD_MIN_BLOCKS : 1;
-  static constexpr int kMinBlocksBwd = kThreads == 256 ? DS_BWD_MIN_BLOCKS : 1;
+  // 128-thread backward (two pixels per thread): 7 CTAs per SM caps it at 70
+  // registers with no spills (93 unbounded, 5 CTAs; bwd 0.488 -> 0.471 ms on
+  // the 1280x720 fit at step 25, B200); 8 CTAs (64 registers) measured slower
+  static constexpr int kMinBlocksBwd = kThreads == 256 ? DS_BWD_MIN_BLOCKS
+                                                        : (kThreads == 128 ? 7 : 1);
   // hits evaluated together: only at 1 pixel per thread; with more pixels the
   // per-pixel state already fills the registers (batch64, B200: grouping
   // at 2 pixels per thread cost 0.6% there and 5% before the backward
