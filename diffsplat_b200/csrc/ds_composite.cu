@@ -179,10 +179,13 @@ __device__ __forceinline__ bool ellipse_hits(const float4& a, const float4& b, f
 }
 
 // Forward alpha of a splat at a pixel (0 when the splat is skipped there):
-// sigma < 0 or beyond the cut, or alpha below 1/255.
+// sigma < 0, or alpha below 1/255.  Beyond the cut (ln(255 o) + 0.01, used by
+// the warp-block tests) alpha is below 0.99 / 255 and fails the threshold test
+// by itself, so the pixel loop does not test sigma against the cut.
 __device__ __forceinline__ float splat_alpha(float dx, float dy, const float4& b, float cut) {
+  (void)cut;
   const float sigma = 0.5f * conic_dist2(dx, dy, b.x, b.y, b.z);
-  if (sigma < 0.f || sigma > cut) return 0.f;
+  if (sigma < 0.f) return 0.f;
   const float alpha = fminf(kMaxAlpha, b.w * __expf(-sigma));
   return alpha < kAlphaThres ? 0.f : alpha;
 }
@@ -627,7 +630,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
             const float sigma = 0.5f * d2g[g];
             eg[g] = __expf(-sigma);
             alg[g] = fminf(kMaxAlpha, bg[g].w * eg[g]);
-            pg[g] = g < ng && batch_end - tg[g] <= fin[k] && !(sigma < 0.f || sigma > cg[g].w) &&
+            pg[g] = g < ng && batch_end - tg[g] <= fin[k] && !(sigma < 0.f) &&
                     !(alg[g] < kAlphaThres);
           }
 #pragma unroll
