@@ -140,15 +140,15 @@ NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.42176e6 / 3085768,
 def kernels_per_step(tiles: int) -> int:
     # step_begin, preprocess, 4 depth-sort passes x 3, count scan x 2, emission,
     # tile sort (grids of up to 8192 tiles: count, offsets + ranges, scatter;
-    # larger: 3 kernels per radix pass over the tile id, then ranges), tile
-    # schedule, composite forward, composite backward (two launches, one per
+    # larger: 3 kernels per radix pass over the tile id, then ranges and the
+    # tile schedule), composite forward, composite backward (two launches, one per
     # pixel layout, each taking its own tiles), long-segment reduce,
     # backward + Adam (which sums the short segments itself)
     if tiles <= 8192:
-        tile_sort = 3
+        tile_sort = 3  # the offsets kernel also writes the tile schedule
     else:
-        tile_sort = 3 * max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8) + 1
-    return 2 + 12 + 2 + 1 + tile_sort + 1 + 1 + 2 + 2
+        tile_sort = 3 * max(1, (max(1, (tiles - 1).bit_length()) + 7) // 8) + 1 + 1
+    return 2 + 12 + 2 + 1 + tile_sort + 1 + 2 + 2
 
 
 def stage_bytes(n: int, isects: int, pixels: int, bands: int = 0) -> dict:

@@ -323,7 +323,8 @@ __global__ void __launch_bounds__(kThreads)
 //   tile_count_kernel   per chunk, pairs per tile -> hist[chunk][tile]
 //   tile_offsets_kernel per tile, exclusive prefix of hist over the chunks
 //                       (in place) and the total; the last CTA to finish
-//                       scans the totals into the tile ranges
+//                       scans the totals into the tile ranges and orders
+//                       the tiles for the composite (longest first)
 //   tile_scatter_kernel per chunk, each warp ranks its run in order (match
 //                       over the lanes' tile ids) and writes every pair to
 //                       range start + chunk prefix + warp prefix + rank.
@@ -366,10 +367,12 @@ __global__ void __launch_bounds__(kThreads)
   for (int t = threadIdx.x; t < tiles; t += kThreads) row[t] = cnt[t];
 }
 
+__device__ void order_tiles(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order);
+
 __global__ void __launch_bounds__(kOffsetThreads)
     tile_offsets_kernel(uint32_t* __restrict__ hist, int chunks, int tiles,
                         uint32_t* __restrict__ totals, int2* __restrict__ ranges,
-                        DevScalars* __restrict__ sc) {
+                        DevScalars* __restrict__ sc, int32_t* __restrict__ order) {
   pdl_wait();
   constexpr int kSlices = kOffsetThreads / 32;
   __shared__ uint32_t part[kSlices][33];
@@ -434,6 +437,11 @@ __global__ void __launch_bounds__(kOffsetThreads)
     base += c;
   }
   if (threadIdx.x == 0) sc->sort_ticket = 0u;
+  if (order) {
+    // the longest-first composite schedule from the ranges just written
+    __syncthreads();
+    order_tiles(ranges, tiles, order);
+  }
 }
 
 // kScatterWarps warps per CTA; dynamic shared memory tiles * (4 + 2 *
@@ -559,9 +567,8 @@ __device__ __forceinline__ int work_bucket(int2 r) {
   return min(kOrderBuckets - 1, 1 + 4 * l + (int)sub);
 }
 
-__global__ void __launch_bounds__(1024)
-    tile_order_kernel(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
-  pdl_wait();
+// The schedule of tiles [0, tiles) from their ranges, by one 1024-thread CTA.
+__device__ void order_tiles(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
   __shared__ uint32_t cnt[kOrderBuckets];
   __shared__ uint32_t off[kOrderBuckets];
   for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0u;
@@ -607,6 +614,12 @@ __global__ void __launch_bounds__(1024)
     base = __shfl_sync(0xffffffffu, base, leader);
     if (b >= 0) order[base + __popc(peers & ((1u << lane) - 1u))] = t;
   }
+}
+
+__global__ void __launch_bounds__(1024)
+    tile_order_kernel(const int2* __restrict__ ranges, int tiles, int32_t* __restrict__ order) {
+  pdl_wait();
+  order_tiles(ranges, tiles, order);
 }
 
 template <typename T>
@@ -828,17 +841,16 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
       const size_t sct_smem = (size_t)T * (4 + 2 * kScatterWarps);
       DS_CUDA(launch_pdl(tile_count_kernel, dim3(G), dim3(kThreads), cnt_smem, s, rb.tile_k0,
                          &sc->n_isects, T, rb.tile_hist, &sc->status));
+      int32_t* order = (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST)
+                           ? rb.tile_order : nullptr;
       DS_CUDA(launch_pdl(tile_offsets_kernel, dim3((T + 31) / 32), dim3(kOffsetThreads), 0, s,
-                         rb.tile_hist, G, T, rb.tile_totals, rb.ranges, sc));
+                         rb.tile_hist, G, T, rb.tile_totals, rb.ranges, sc, order));
       DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * kScatterWarps), sct_smem, s,
                          rb.tile_k0,
                          rb.emit_splat, &sc->n_isects, T, rb.tile_hist, rb.ranges,
                          rb.sorted_splat, rb.tile_v0));
       rb.sorted_emit = rb.tile_v0;
       rb.sorted_tile = nullptr;
-      if (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST)
-        DS_CUDA(launch_pdl(tile_order_kernel, dim3(1), dim3(1024), 0, s, rb.ranges, rb.tiles,
-                           rb.tile_order));
       if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
       return cuda_status(cudaGetLastError());
     }
