@@ -139,6 +139,7 @@ _SIGS = {
     "ds_fitter_step": (C.c_int, [_vp, C.c_int, _vp]),
     "ds_fitter_loss": (C.c_int, [_vp, C.POINTER(C.c_float), _vp]),
     "ds_fitter_output": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "ds_fitter_loss_device": (C.c_int, [_vp, C.POINTER(_vp)]),
     "ds_fitter_step_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "ds_fitter_status": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
     "ds_fitter_destroy": (C.c_int, [_vp]),

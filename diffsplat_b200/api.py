@@ -333,6 +333,12 @@ class Fitter:
         L.call("ds_fitter_output", self.h, C.byref(p))
         return _wrap_device(p.value, (self.height, self.width, 3))
 
+    def loss_device(self) -> torch.Tensor:
+        """The device scalar each step writes its loss to (float32 [1] view)."""
+        p = C.c_void_p()
+        L.call("ds_fitter_loss_device", self.h, C.byref(p))
+        return _wrap_device(p.value, (1,))
+
     def grads(self) -> torch.Tensor:
         g = L.Gaussian3D()
         L.call("ds_fitter_grads", self.h, C.byref(g))

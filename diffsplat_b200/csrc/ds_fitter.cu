@@ -327,6 +327,12 @@ int ds_fitter_loss(ds_fitter* f, float* loss, ds_stream stream) {
   return DS_OK;
 }
 
+int ds_fitter_loss_device(ds_fitter* f, float** loss) {
+  if (!f || !loss) return DS_ERR_ARG;
+  *loss = &f->rb.scalars->loss;
+  return DS_OK;
+}
+
 int ds_fitter_output(ds_fitter* f, float** image) {
   if (!f || !image) return DS_ERR_ARG;
   *image = f->image;

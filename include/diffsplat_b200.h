@@ -264,6 +264,9 @@ int ds_fitter_set_camera(ds_fitter *f, const float pv[16], const float cam_pos[3
 int ds_fitter_step(ds_fitter *f, int n_steps, ds_stream stream);
 /* Loss of the most recent step's forward (synchronises the stream). */
 int ds_fitter_loss(ds_fitter *f, float *loss, ds_stream stream);
+/* Device address of the loss scalar each step writes (float): lets a caller
+ * copy it asynchronously, e.g. read step k's loss while step k + 1 runs. */
+int ds_fitter_loss_device(ds_fitter *f, float **loss);
 /* Device pointer of the rendered image [H*W*3] of the most recent forward. */
 int ds_fitter_output(ds_fitter *f, float **image);
 int ds_fitter_step_count(ds_fitter *f, int *out);
