@@ -134,11 +134,11 @@ def fp32_peak_tflops(sm_mhz: float) -> float:
 FLOPS_PER_PAIR = {"composite_fwd": 24, "composite_bwd": 70}
 
 # DRAM bytes (read + write) per (tile, splat) pair of one composite launch, from
-# one ncu capture of the same 1280x720 / 60000-splat workload (profile run, step
-# 21, about 3,085,768 pairs: forward 22.42 MB, backward 184.27 MB), scaled by
+# one ncu capture of the same 1280x720 / 60000-splat workload (profile run,
+# step 21, 3,085,820 pairs: forward 22.40 MB, backward 63.35 MB), scaled by
 # the bench's own pair count.
-NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.42176e6 / 3085768,
-                            "composite_bwd": 184.27365e6 / 3085768}
+NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.396416e6 / 3085820,
+                            "composite_bwd": (50.629632e6 + 12.717056e6) / 3085820}
 
 
 def kernels_per_step(tiles: int) -> int:
@@ -318,11 +318,28 @@ def run_reference(args, world, rank, local):
 
 def profile_run(args):
     """Eager (non-graph) steps of the bench workload for profilers: every kernel
-    is a separate launch, device memory stays under 1 GB."""
+    is a separate launch, device memory stays under 1 GB.  With --workload
+    viewer-sh3: eager fitter steps of the 1M-splat SH-3 scene at 1920x1080
+    from its first orbit camera (about 2 GB)."""
     import torch
     from diffsplat_b200 import api
     from diffsplat_b200.scenes import reference_default
     torch.cuda.set_device(0)
+    if args.workload == "viewer-sh3":
+        from diffsplat_b200.scenes import make_target, orbit_cameras, viewer_scene
+        W, H, n = 1920, 1080, 1_000_000
+        f = api.Fitter(W, H, n, 3, max_isects=1 << 23, use_graph=False)
+        f.set_params(torch.tensor(viewer_scene(n, seed=0), device="cuda"))
+        f.set_target(torch.tensor(make_target(W, H, 2000, 7), device="cuda"))
+        f.set_camera(*orbit_cameras(16, width=W, height=H, fx=1200.0)[0])
+        f.step(args.warmup + args.steps)
+        torch.cuda.synchronize()
+        code, _ = f.status()
+        print(f"profile run (viewer-sh3): {args.warmup + args.steps} steps, status {code}")
+        f.close()
+        if code != 0:
+            sys.exit(1)
+        return
     prob = reference_default(seed=0)
     f = api.Fitter(prob.width, prob.height, prob.params.shape[1], prob.sh_degree, lrs=prob.lrs,
                    max_isects=1 << 22, use_graph=False)
