@@ -43,7 +43,7 @@ constexpr int kBwdGroupPpt1 = DS_BWD_GROUP;  // backward hits evaluated together
 #define DS_FWD_MIN_BLOCKS 4
 #endif
 #ifndef DS_BWD_MIN_BLOCKS
-#define DS_BWD_MIN_BLOCKS 4
+#define DS_BWD_MIN_BLOCKS 3
 #endif
 
 // Backward layout chosen per forward when ppt_bwd is 0: two pixels per thread
@@ -70,7 +70,9 @@ struct Lay {
   static constexpr int kMinBlocksFwd = kThreads == 256 ? DS_FWD_MIN_BLOCKS : 1;
   // 128-thread backward (two pixels per thread): 7 CTAs per SM caps it at 70
   // registers with no spills (93 unbounded, 5 CTAs; bwd 0.488 -> 0.471 ms on
-  // the 1280x720 fit at step 25, B200); 8 CTAs (64 registers) measured slower
+  // the 1280x720 fit at step 25, B200); 8 CTAs (64 registers) measured slower.
+  // 256-thread backward (one pixel per thread): 3 CTAs per SM (up to 85
+  // registers); at 4 (64 registers) it spills, 0.479 -> 0.503 ms at step 1010
   static constexpr int kMinBlocksBwd = kThreads == 256 ? DS_BWD_MIN_BLOCKS
                                                         : (kThreads == 128 ? 7 : 1);
   // hits evaluated together: only at 1 pixel per thread; with more pixels the
@@ -443,7 +445,8 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
     composite_bwd_kernel(const float4* __restrict__ ra, const float4* __restrict__ rb,
                          const float4* __restrict__ rc, const float* __restrict__ ridet,
                          const uint32_t* __restrict__ sorted_splat,
-                         const uint32_t* __restrict__ sorted_emit, const int2* __restrict__ ranges,
+                         const uint32_t* __restrict__ seg_start,
+                         const ushort4* __restrict__ rect, const int2* __restrict__ ranges,
                          const int32_t* __restrict__ order, const float* __restrict__ alphas,
                          const int32_t* __restrict__ last_ids,
                          const float* __restrict__ grad_or_image, const float* __restrict__ target,
@@ -460,6 +463,8 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   constexpr int B = Lc::kBwdBatch;
   __shared__ float4 sA[B], sB[B], sC[B];
   __shared__ float sI[B];
+  __shared__ uint32_t sG[2][B];  // splat ids of the staged batch and the next
+  __shared__ int sRC[2];
   __shared__ uint32_t sMask[B];
   __shared__ float4 sBox[NW];
   __shared__ __align__(16) float part[NW][B * 9];  // per-warp partial of each batch splat
@@ -478,6 +483,10 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
   const int W = tg.W, H = tg.H;
   const Pixels<PPT> m = pixels<PPT, TS>(tg.local, tg.ntx, W, H);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {  // the tile's row and column in its grid, for the record indices
+    sRC[0] = tg.local / tg.ntx;
+    sRC[1] = tg.local - sRC[0] * tg.ntx;
+  }
   if (lane == 0) sBox[w] = make_float4(m.wx_lo, m.wx_hi, m.wy_lo, m.wy_hi);
   // acc[k]: over the splats behind (already visited), weight x (colour . dL/dpixel)
   float T[PPT], gr[PPT], gg[PPT], gb[PPT], acc[PPT];
@@ -542,6 +551,7 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
         pf[r].b = rb[g];
         pf[r].c = rc[g];
         pf[r].idet = ridet[g];
+        if ((threadIdx.x + r * NT) % kSplit == 0) sG[bi & 1][l] = g;
       }
     }
   };
@@ -696,9 +706,15 @@ __global__ void __launch_bounds__(Lay<PPT, TS>::kThreads, Lay<PPT, TS>::kMinBloc
       }
     }
     __syncthreads();
+    const int trow = sRC[0], tcol = sRC[1];
     for (int slot = threadIdx.x; slot < bs * kSplit; slot += NT) {
       const int l = slot / kSplit, h = slot % kSplit;
-      const uint32_t e = sorted_emit[batch_end - l];
+      // the pair's emission index: the splat's first one plus the tile's
+      // row-major index in the splat's tile rectangle
+      const uint32_t g = sG[bi & 1][l];
+      const ushort4 r = rect[g];
+      const uint32_t e = seg_start[g] + (uint32_t)(trow - r.z) * (uint32_t)(r.y - r.x + 1) +
+                         (uint32_t)(tcol - r.x);
       float* dst = isect_grad + (size_t)e * 9;
 #pragma unroll
       for (int q = h; q < 9; q += kSplit) {
@@ -747,7 +763,7 @@ void launch_bwd(RasterBuffers& rb, const float* image, const float* grad_rgb, co
   const int32_t* order = schedule(rb);
 #define DS_BWD(F, E)                                                                         \
   launch_pdl(composite_bwd_kernel<PPT, TS, F, E, kBatch>, dim3(rb.tiles), dim3(NT), 0, s,     \
-             rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.sorted_emit,      \
+             rb.rec_a, rb.rec_b, rb.rec_c, rb.rec_idet, rb.sorted_splat, rb.seg_start, rb.rect,\
              rb.ranges, order, rb.alphas, rb.last_ids, g, t, rb.isect_grad, rb.width,         \
              rb.height, rb.ntx, rb.tile_inst, rb.geom, rb.depth_keys, rb.tile_bound, mode)
   if (grad_rgb) {

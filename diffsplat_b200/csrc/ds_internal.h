@@ -224,7 +224,7 @@ struct RasterBuffers {
 
   // results of the last sort (point into the ping-pong buffers)
   uint32_t* sorted_tile = nullptr;
-  uint32_t* sorted_emit = nullptr;
+  uint32_t* sorted_emit = nullptr;  // radix path: emission index of each sorted pair
   uint32_t* depth_perm = nullptr;         // depth-sorted splat ids
   uint32_t* depth_sorted_keys = nullptr;  // their depth keys
 

@@ -326,8 +326,11 @@ __global__ void __launch_bounds__(kThreads)
 //                       scans the totals into the tile ranges and orders
 //                       the tiles for the composite (longest first)
 //   tile_scatter_kernel per chunk, each warp ranks its run in order (match
-//                       over the lanes' tile ids) and writes every pair to
-//                       range start + chunk prefix + warp prefix + rank.
+//                       over the lanes' tile ids) and writes every pair's
+//                       splat id to range start + chunk prefix + warp
+//                       prefix + rank.  (The composite backward finds a
+//                       pair's emission index from the splat's first one and
+//                       the tile's place in its rectangle, so none is stored.)
 // One pass over the pairs instead of ceil(log2 T / 8) radix passes, and the
 // ranges come out of the scan.
 constexpr int kOffsetThreads = 1024;  // 32 tiles x 32 slices of the chunk column
@@ -456,8 +459,7 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
     tile_scatter_kernel(const uint32_t* __restrict__ tile_keys,
                         const uint32_t* __restrict__ emit_splat, const uint32_t* __restrict__ n_dev,
                         int tiles, const uint32_t* __restrict__ hist,
-                        const int2* __restrict__ ranges, uint32_t* __restrict__ sorted_splat,
-                        uint32_t* __restrict__ sorted_emit) {
+                        const int2* __restrict__ ranges, uint32_t* __restrict__ sorted_splat) {
   pdl_wait();
   extern __shared__ uint32_t smem[];
   constexpr int NT = 32 * kScatterWarps;
@@ -543,11 +545,7 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
         }
       }
       p0 = __shfl_sync(0xffffffffu, p0, leader);
-      if (valid) {
-        const uint32_t pos = p0 + __popc(peers & lt);
-        sorted_splat[pos] = sp[u];
-        sorted_emit[pos] = e0 + 32 * u + lane;
-      }
+      if (valid) sorted_splat[p0 + __popc(peers & lt)] = sp[u];
       __syncwarp();
     }
   }
@@ -848,8 +846,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
       DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * kScatterWarps), sct_smem, s,
                          rb.tile_k0,
                          rb.emit_splat, &sc->n_isects, T, rb.tile_hist, rb.ranges,
-                         rb.sorted_splat, rb.tile_v0));
-      rb.sorted_emit = rb.tile_v0;
+                         rb.sorted_splat));
       rb.sorted_tile = nullptr;
       if (ev) DS_CUDA(cudaEventRecord(ev[2], s));
       return cuda_status(cudaGetLastError());
