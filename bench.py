@@ -135,10 +135,10 @@ FLOPS_PER_PAIR = {"composite_fwd": 24, "composite_bwd": 70}
 
 # DRAM bytes (read + write) per (tile, splat) pair of one composite launch, from
 # one ncu capture of the same 1280x720 / 60000-splat workload (profile run,
-# step 21, 3,085,820 pairs: forward 22.40 MB, backward 63.35 MB), scaled by
+# step 21, 3,085,820 pairs: forward 22.40 MB, backward 59.55 MB), scaled by
 # the bench's own pair count.
 NCU_DRAM_BYTES_PER_ISECT = {"composite_fwd": 22.396416e6 / 3085820,
-                            "composite_bwd": (50.629632e6 + 12.717056e6) / 3085820}
+                            "composite_bwd": (47.626240e6 + 11.928064e6) / 3085820}
 
 
 def kernels_per_step(tiles: int) -> int:
