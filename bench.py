@@ -103,12 +103,14 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(world, value: float) -> float:
+def max_over_ranks(world, value: float, device: str = "cuda") -> float:
+    """The largest `value` over the ranks (the process group's backend must
+    reduce tensors on `device`: NCCL on "cuda", gloo on "cpu")."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    t = torch.tensor([value], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
