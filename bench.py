@@ -359,6 +359,74 @@ def profile_run(args):
         sys.exit(1)
 
 
+def run_isects(args) -> dict:
+    """(tile, splat) pairs I per splat N of every config, from this build's
+    forward (whose pair counts equal the reference's: the parity tests compare
+    them bit for bit): c0 and c1 at the fit's initial state and, for c1, after
+    25 and 1010 steps; c2 for each of the 16 orbit cameras; c3 per instance at
+    its initial state; c4 for random splats on 512^2 targets."""
+    import torch
+    from diffsplat_b200 import api
+    from diffsplat_b200.scenes import (batch_problems, orbit_cameras, plain_small,
+                                       reference_default, small_problem, viewer_scene)
+    torch.cuda.set_device(0)
+
+    def render_pairs(prob, max_isects=0):
+        r = api.Renderer(prob.width, prob.height, prob.params.shape[1], prob.sh_degree,
+                         max_isects=max_isects)
+        r.set_params(torch.tensor(prob.params, device="cuda").contiguous())
+        r.render(prob.pv, prob.cam)
+        torch.cuda.synchronize()
+        c = r.counts()
+        r.close()
+        return c
+
+    out = {}
+    for name, prob in [("c0 256x256, 4096 splats", plain_small(0)),
+                       ("c1 1280x720, 60000 splats", reference_default(0)),
+                       ("c4 512x512, 16384 random splats", small_problem(512, 512, 16384, 0))]:
+        c = render_pairs(prob)
+        n = prob.params.shape[1]
+        out[name] = {"N": n, "I": c["n_isects"], "I_per_N": c["n_isects"] / n,
+                     "visible": c["visible"]}
+    prob = reference_default(0)
+    n = prob.params.shape[1]
+    f = api.Fitter(prob.width, prob.height, n, prob.sh_degree, lrs=prob.lrs)
+    f.set_params(prob.params)
+    f.set_target(torch.tensor(prob.target, device="cuda"))
+    f.set_camera(prob.pv, prob.cam)
+    fit, done = {}, 0
+    for k in (25, 1010):
+        f.step(k - done)
+        done = k
+        c = f.counters()
+        fit[f"step {k}"] = {"I": c["n_isects"], "I_per_N": c["n_isects"] / n}
+    f.close()
+    out["c1 1280x720, 60000 splats"]["fit"] = fit
+    P = viewer_scene()
+    n = P.shape[1]
+    r = api.Renderer(1920, 1080, n, 3)
+    r.set_params(torch.tensor(P, device="cuda").contiguous())
+    per_cam = []
+    for pv, eye in orbit_cameras():
+        r.render(pv, eye)
+        torch.cuda.synchronize()
+        per_cam.append(r.counts()["n_isects"])
+    r.close()
+    out["c2 1920x1080, 1M splats, SH 3"] = {"N": n, "I_per_camera": per_cam,
+                                            "I_per_N_mean": float(np.mean(per_cam)) / n}
+    inst = []
+    for prob in batch_problems():
+        c = render_pairs(prob)
+        inst.append((prob.width, prob.height, prob.params.shape[1], c["n_isects"]))
+    out["c3 64 instances"] = {
+        "I_total": sum(x[3] for x in inst), "N_total": sum(x[2] for x in inst),
+        "I_per_N_min": min(x[3] / x[2] for x in inst),
+        "I_per_N_max": max(x[3] / x[2] for x in inst),
+        "instances": [{"W": w, "H": h, "N": m, "I": i} for w, h, m, i in inst]}
+    return out
+
+
 def run_viewer(args) -> dict:
     """Viewer-style SH-3 scene: 1M splats, 1920x1080, 16 orbit cameras (fx 1200).
     Forward-only renders (the SplatRenderer path) and fwd+bwd+Adam fitter steps,
@@ -617,12 +685,13 @@ def main():
                          "2^22-pair buffer (for ncu captures); prints no JSON line")
     ap.add_argument("--gemm", default=None, metavar="M,N,K",
                     help="time one BF16 tensor-core GEMM shape and print its TFLOP/s")
-    ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64", "init"],
+    ap.add_argument("--workload", choices=["fitter", "viewer-sh3", "batch64", "init", "isects"],
                     default="fitter",
                     help="fitter: the headline 1280x720 / 60000-splat training step; "
                          "viewer-sh3: 1M-splat SH-3 scene at 1920x1080, forward and fwd+bwd; "
                          "batch64: 64 uneven instances in one batched step vs sequential; "
-                         "init: learned initializer training and seconds to 28 dB")
+                         "init: learned initializer training and seconds to 28 dB; "
+                         "isects: (tile, splat) pairs per splat of every config (untimed)")
     args = ap.parse_args()
     if args.profile_run:
         profile_run(args)
@@ -634,6 +703,10 @@ def main():
         tf = gemm_tflops(M, N, K, reps=max(1, args.steps))
         print(json.dumps({"metric": "tcgen05 BF16 GEMM TFLOP/s", "M": M, "N": N, "K": K,
                           "value": tf, "unit": "TFLOP/s"}))
+        return
+    if args.workload == "isects":
+        print(json.dumps({"metric": "(tile, splat) pairs per splat, per config",
+                          "data": "synthetic", **run_isects(args)}))
         return
     if args.workload == "init":
         res = run_init(args)
