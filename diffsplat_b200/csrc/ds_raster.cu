@@ -74,8 +74,9 @@ __global__ void __launch_bounds__(kThreads)
                 const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom,
                 int2* __restrict__ ranges, int tiles) {
   pdl_wait();
-  // The tile ranges of this forward start empty (ranges_kernel fills the
-  // non-empty ones after the tile sort).
+  // The tile ranges of this forward start empty: after the radix tile sort
+  // ranges_kernel fills only the non-empty ones (the counting sort's scan
+  // writes every tile's).
   for (int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x; q < tiles;
        q += (int64_t)gridDim.x * kThreads)
     ranges[q] = make_int2(0, 0);
