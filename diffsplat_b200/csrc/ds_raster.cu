@@ -66,10 +66,13 @@ __global__ void __launch_bounds__(kThreads)
   count_visible(vis, &sc->visible);
 }
 
+// TK: the tile id's type, 16 bits on the counting path (at most
+// kCountSortMaxTiles tiles), 32 for the radix passes.
+template <typename TK>
 __global__ void __launch_bounds__(kThreads)
     emit_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ counts,
                 const unsigned long long* __restrict__ offsets, const ushort4* __restrict__ rect,
-                int n, int ntx, uint32_t cap, uint32_t* __restrict__ tile_keys,
+                int n, int ntx, uint32_t cap, TK* __restrict__ tile_keys,
                 uint32_t* __restrict__ emit_splat, uint32_t* __restrict__ seg_start,
                 const uint16_t* __restrict__ inst_of_splat, const InstGeom* __restrict__ geom,
                 int2* __restrict__ ranges, int tiles) {
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t row0 = base + y0 * pitch + x0;
     for (uint32_t k = q; k < m; k += 4) {
       const uint32_t ty = row_of(k, w, inv);
-      tile_keys[off + k] = row0 + ty * pitch + (k - ty * w);
+      tile_keys[off + k] = (TK)(row0 + ty * pitch + (k - ty * w));
       emit_splat[off + k] = i;
     }
   }
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t row0 = sb + sy * sp + sx;
     for (uint32_t k = lane; k < sm; k += 32) {
       const uint32_t ty = row_of(k, sw, sinv);
-      tile_keys[soff + k] = row0 + ty * sp + (k - ty * sw);
+      tile_keys[soff + k] = (TK)(row0 + ty * sp + (k - ty * sw));
       emit_splat[soff + k] = si;
     }
   }
@@ -344,7 +347,7 @@ __device__ __forceinline__ void chunk_of(uint32_t n, uint32_t chunks, uint32_t c
 }
 
 __global__ void __launch_bounds__(kThreads)
-    tile_count_kernel(const uint32_t* __restrict__ tile_keys, const uint32_t* __restrict__ n_dev,
+    tile_count_kernel(const uint16_t* __restrict__ tile_keys, const uint32_t* __restrict__ n_dev,
                       int tiles, uint32_t* __restrict__ hist, uint32_t* __restrict__ status) {
   pdl_wait();
   extern __shared__ uint32_t cnt[];  // [tiles]
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int u = 0; u < kAhead; ++u) {
       const uint32_t e = e0 + u * kThreads;
-      tk[u] = e < hi ? tile_keys[e] : 0xfffffffeu;
+      tk[u] = e < hi ? (uint32_t)tile_keys[e] : 0xfffffffeu;
     }
 #pragma unroll
     for (int u = 0; u < kAhead; ++u) {
@@ -457,7 +460,7 @@ constexpr int kScatterWarps = 8;
 constexpr uint32_t kScatterChunk16 = 65535;
 
 __global__ void __launch_bounds__(32 * kScatterWarps)
-    tile_scatter_kernel(const uint32_t* __restrict__ tile_keys,
+    tile_scatter_kernel(const uint16_t* __restrict__ tile_keys,
                         const uint32_t* __restrict__ emit_splat, const uint32_t* __restrict__ n_dev,
                         int tiles, const uint32_t* __restrict__ hist,
                         const int2* __restrict__ ranges, uint32_t* __restrict__ sorted_splat) {
@@ -495,7 +498,7 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
 #pragma unroll
       for (int u = 0; u < kAhead; ++u) {
         const uint32_t e = e0 + 32 * u + lane;
-        tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
+        tk[u] = e < whi ? (uint32_t)tile_keys[e] : 0xffffffffu;
       }
 #pragma unroll
       for (int u = 0; u < kAhead; ++u) {
@@ -525,7 +528,7 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
 #pragma unroll
     for (int u = 0; u < kAhead; ++u) {
       const uint32_t e = e0 + 32 * u + lane;
-      tk[u] = e < whi ? tile_keys[e] : 0xffffffffu;
+      tk[u] = e < whi ? (uint32_t)tile_keys[e] : 0xffffffffu;
       sp[u] = e < whi ? emit_splat[e] : 0u;
     }
 #pragma unroll
@@ -828,24 +831,33 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
                                 &sc->n_isects, &sc->n_isects_raw, (uint32_t)rb.cap, &sc->status,
                                 rb.scan, s, with_long_list ? rb.long_list : nullptr, &sc->n_long));
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
-    DS_CUDA(launch_pdl(emit_kernel, dim3((unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads)),
-                       dim3(kThreads), 0, s, rb.depth_perm, rb.counts, rb.emit_offsets, rb.rect,
-                       n, rb.ntx, (uint32_t)rb.cap, rb.tile_k0, rb.emit_splat, rb.seg_start,
-                       rb.inst_of_splat, rb.geom, rb.ranges, rb.tiles));
+    const dim3 emit_grid((unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads));
+    uint16_t* tile16 = reinterpret_cast<uint16_t*>(rb.tile_k0);  // counting path
+    if (rb.tile_hist) {
+      DS_CUDA(launch_pdl(emit_kernel<uint16_t>, emit_grid, dim3(kThreads), 0, s, rb.depth_perm,
+                         rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap, tile16,
+                         rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom, rb.ranges,
+                         rb.tiles));
+    } else {
+      DS_CUDA(launch_pdl(emit_kernel<uint32_t>, emit_grid, dim3(kThreads), 0, s, rb.depth_perm,
+                         rb.counts, rb.emit_offsets, rb.rect, n, rb.ntx, (uint32_t)rb.cap,
+                         rb.tile_k0, rb.emit_splat, rb.seg_start, rb.inst_of_splat, rb.geom,
+                         rb.ranges, rb.tiles));
+    }
     if (ev) DS_CUDA(cudaEventRecord(ev[1], s));
     if (rb.tile_hist) {
       // 4) stable counting sort by tile id; the ranges come out of its scan
       const int T = rb.tiles, G = rb.count_chunks;
       const size_t cnt_smem = (size_t)T * 4;
       const size_t sct_smem = (size_t)T * (4 + 2 * kScatterWarps);
-      DS_CUDA(launch_pdl(tile_count_kernel, dim3(G), dim3(kThreads), cnt_smem, s, rb.tile_k0,
+      DS_CUDA(launch_pdl(tile_count_kernel, dim3(G), dim3(kThreads), cnt_smem, s, tile16,
                          &sc->n_isects, T, rb.tile_hist, &sc->status));
       int32_t* order = (rb.tile_order && rb.schedule == DS_SCHEDULE_LONGEST_FIRST)
                            ? rb.tile_order : nullptr;
       DS_CUDA(launch_pdl(tile_offsets_kernel, dim3((T + 31) / 32), dim3(kOffsetThreads), 0, s,
                          rb.tile_hist, G, T, rb.tile_totals, rb.ranges, sc, order));
       DS_CUDA(launch_pdl(tile_scatter_kernel, dim3(G), dim3(32 * kScatterWarps), sct_smem, s,
-                         rb.tile_k0,
+                         tile16,
                          rb.emit_splat, &sc->n_isects, T, rb.tile_hist, rb.ranges,
                          rb.sorted_splat));
       rb.sorted_tile = nullptr;
