@@ -834,6 +834,7 @@ int raster_build_lists(RasterBuffers& rb, int n, cudaStream_t s, cudaEvent_t* ev
                                 rb.scan, s, with_long_list ? rb.long_list : nullptr, &sc->n_long));
     // 3) emit (tile, emission index) pairs grouped by splat in depth order
     const dim3 emit_grid((unsigned)(((int64_t)n * 4 + kThreads - 1) / kThreads));
+    static_assert(kCountSortMaxTiles <= 65536, "counting-path tile ids are 16-bit");
     uint16_t* tile16 = reinterpret_cast<uint16_t*>(rb.tile_k0);  // counting path
     if (rb.tile_hist) {
       DS_CUDA(launch_pdl(emit_kernel<uint16_t>, emit_grid, dim3(kThreads), 0, s, rb.depth_perm,
