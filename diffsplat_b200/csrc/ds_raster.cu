@@ -541,22 +541,40 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
 #pragma unroll
     for (int u = 0; u < kAhead; ++u) {
       const uint32_t t = tk[u];
-      const uint32_t peers = __match_any_sync(0xffffffffu, t);
-      const int leader = __ffs(peers) - 1;
       const bool valid = t < (uint32_t)tiles;  // false past the run's end
-      uint32_t p0 = 0;
-      if (valid && lane == leader) {
-        const uint32_t n_peers = (uint32_t)__popc(peers);
-        if (big) {
-          p0 = base[t] + wide[t];
-          wide[t] += n_peers;
-        } else {
-          p0 = base[t] + mine[t];
-          mine[t] = (uint16_t)(mine[t] + n_peers);
+      if (__all_sync(0xffffffffu, sp[u] == __shfl_sync(0xffffffffu, sp[u], 0))) {
+        // all 32 pairs of the step come from one splat, whose tiles are
+        // distinct: each pair is the first of its tile here, no ranking is
+        // needed (most steps, the pairs being grouped by splat; tile sort
+        // 0.058 -> 0.054 ms at step 25 of the 1280x720 / 60000-splat fit)
+        if (valid) {
+          uint32_t p;
+          if (big) {
+            p = base[t] + wide[t];
+            wide[t] += 1u;
+          } else {
+            p = base[t] + mine[t];
+            mine[t] = (uint16_t)(mine[t] + 1u);
+          }
+          sorted_splat[p] = sp[u];
         }
+      } else {
+        const uint32_t peers = __match_any_sync(0xffffffffu, t);
+        const int leader = __ffs(peers) - 1;
+        uint32_t p0 = 0;
+        if (valid && lane == leader) {
+          const uint32_t n_peers = (uint32_t)__popc(peers);
+          if (big) {
+            p0 = base[t] + wide[t];
+            wide[t] += n_peers;
+          } else {
+            p0 = base[t] + mine[t];
+            mine[t] = (uint16_t)(mine[t] + n_peers);
+          }
+        }
+        p0 = __shfl_sync(0xffffffffu, p0, leader);
+        if (valid) sorted_splat[p0 + __popc(peers & lt)] = sp[u];
       }
-      p0 = __shfl_sync(0xffffffffu, p0, leader);
-      if (valid) sorted_splat[p0 + __popc(peers & lt)] = sp[u];
       __syncwarp();
     }
   }
