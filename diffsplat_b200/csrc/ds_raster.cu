@@ -583,7 +583,8 @@ __global__ void __launch_bounds__(32 * kScatterWarps)
 // Longest-first schedule of the composite CTAs: tiles bucketed by their list
 // length (quarter-octave buckets), buckets in descending order.  The heaviest
 // tiles start in the first wave, so they no longer set the kernel's tail.  The
-// order inside a bucket is arbitrary; every tile's result is independent of it.
+// order inside a bucket is arbitrary (plain shared atomics hand out the
+// slots); every tile's result is independent of it.
 constexpr int kOrderBuckets = 128;
 
 __device__ __forceinline__ int work_bucket(int2 r) {
@@ -604,9 +605,7 @@ __device__ void order_tiles(const int2* __restrict__ ranges, int tiles, int32_t*
   const int rounds = (tiles + (int)blockDim.x - 1) / (int)blockDim.x;
   for (int r = 0; r < rounds; ++r) {
     const int t = r * blockDim.x + threadIdx.x;
-    const int b = t < tiles ? work_bucket(ranges[t]) : -1;
-    const uint32_t peers = __match_any_sync(0xffffffffu, b);
-    if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[b], (uint32_t)__popc(peers));
+    if (t < tiles) atomicAdd(&cnt[work_bucket(ranges[t])], 1u);
   }
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -633,13 +632,7 @@ __device__ void order_tiles(const int2* __restrict__ ranges, int tiles, int32_t*
   __syncthreads();
   for (int r = 0; r < rounds; ++r) {
     const int t = r * blockDim.x + threadIdx.x;
-    const int b = t < tiles ? work_bucket(ranges[t]) : -1;
-    const uint32_t peers = __match_any_sync(0xffffffffu, b);
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if (b >= 0 && lane == leader) base = atomicAdd(&off[b], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (b >= 0) order[base + __popc(peers & ((1u << lane) - 1u))] = t;
+    if (t < tiles) order[atomicAdd(&off[work_bucket(ranges[t])], 1u)] = t;
   }
 }
 

@@ -58,8 +58,13 @@ __global__ void __launch_bounds__(kThreads)
     }
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-      const uint32_t peers = __match_any_sync(0xffffffffu, d[it]);
-      if (d[it] < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d[it]], (uint32_t)__popc(peers));
+      // one atomic for a warp whose 32 keys share the digit (the high digits
+      // of depth keys nearly always do), else one per key
+      if (__all_sync(0xffffffffu, d[it] == __shfl_sync(0xffffffffu, d[it], 0))) {
+        if (d[it] < 256u && lane == 0) atomicAdd(&h[d[it]], 32u);
+      } else if (d[it] < 256u) {
+        atomicAdd(&h[d[it]], 1u);
+      }
     }
   }
   __syncthreads();
@@ -159,7 +164,9 @@ __global__ void __launch_bounds__(kThreads)
       const uint32_t idx = t0 + w * 256 + it * 32 + lane;
       const bool ok = idx < end;
       const uint32_t d = ok ? ((key[it] >> shift) & 255u) : 0x100u;
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      // a warp whose 32 keys share the digit ranks them by lane, no match
+      const uint32_t peers = __all_sync(0xffffffffu, d == __shfl_sync(0xffffffffu, d, 0))
+                                 ? 0xffffffffu : __match_any_sync(0xffffffffu, d);
       const uint32_t pre = ok ? cnt[w][d] : 0u;
       __syncwarp();
       if (ok && lane == __ffs(peers) - 1) cnt[w][d] = pre + __popc(peers);
